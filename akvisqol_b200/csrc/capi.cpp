@@ -1,0 +1,399 @@
+// C ABI of libvisqol (include/visqol.h, include/visqol_b200.h).
+//
+// Mirrors the reference's src/capi.zig:119-456: options with defaults,
+// thread-local last-error text, heap-boxed results that own their arrays,
+// per-pair status in batches (the first error is the return value), and
+// files grouped by sample rate. The engine behind it is the GPU pipeline;
+// there is no CPU fallback.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/visqol.h"
+#include "../../include/visqol_b200.h"
+#include "engine.h"
+#include "host_model.h"
+
+using vqb::Error;
+
+struct visqol_ctx {
+    vqb::Options opt;
+    std::shared_ptr<const vqb::host::Svr> svr;
+    std::unique_ptr<vqb::Engine> engine;
+};
+
+namespace {
+
+// The calling thread's last error, 512 bytes as the reference's
+// (src/capi.zig:85-91).
+thread_local char g_error[512] = {0};
+
+void set_error(const std::string &m) { std::snprintf(g_error, sizeof g_error, "%s", m.c_str()); }
+
+int fail(int code, const std::string &m) {
+    set_error(m);
+    return code;
+}
+
+// A result and the storage its pointers view (reference src/capi.zig:66-70).
+struct Box {
+    visqol_result c{};
+    vqb::host::Scores s;
+    std::vector<double> band_data;
+    std::vector<visqol_patch> patches;
+};
+
+visqol_result *box_scores(vqb::host::Scores &&s) {
+    auto *b = new Box();
+    b->s = std::move(s);
+    const size_t nb = b->s.fvnsim.size(), np = b->s.patches.size();
+    b->band_data.resize(np * nb * 3);
+    b->patches.resize(np);
+    for (size_t i = 0; i < np; ++i) {
+        const auto &m = b->s.patches[i];
+        double *dst = b->band_data.data() + i * nb * 3;
+        std::copy(m.means.begin(), m.means.end(), dst);
+        std::copy(m.stddevs.begin(), m.stddevs.end(), dst + nb);
+        std::copy(m.energy.begin(), m.energy.end(), dst + 2 * nb);
+        b->patches[i] = visqol_patch{m.similarity, m.ref_start, m.ref_end, m.deg_start, m.deg_end,
+                                     dst, dst + nb, dst + 2 * nb};
+    }
+    b->c.moslqo = b->s.moslqo;
+    b->c.vnsim = b->s.vnsim;
+    b->c.alignment_lag_s = b->s.lag_s;
+    b->c.num_bands = nb;
+    b->c.fvnsim = b->s.fvnsim.data();
+    b->c.fvnsim10 = b->s.fvnsim10.data();
+    b->c.fstdnsim = b->s.fstdnsim.data();
+    b->c.fvdegenergy = b->s.fvdegenergy.data();
+    b->c.center_freq_bands = b->s.cf.data();
+    b->c.num_patches = np;
+    b->c.patch_sims = b->patches.data();
+    return &b->c;
+}
+
+struct TraceBox {
+    visqol_b200_trace c{};
+    vqb::PairTrace t;
+};
+
+visqol_b200_trace *box_trace(vqb::PairTrace &&t) {
+    auto *b = new TraceBox();
+    b->t = std::move(t);
+    visqol_b200_trace &c = b->c;
+    c.global_lag = b->t.global_lag;
+    c.spl_factor = b->t.spl_factor;
+    c.deg_len = b->t.deg_len;
+    c.nf_ref = b->t.nf_ref;
+    c.nf_deg = b->t.nf_deg;
+    c.num_patches = b->t.ref_index.size();
+    c.ref_index = b->t.ref_index.data();
+    c.deg_offset = b->t.deg_offset.data();
+    c.valid = b->t.valid.data();
+    c.realign_lag = b->t.realign_lag.data();
+    c.realign_frames = b->t.realign_frames.data();
+    c.realign_reused = b->t.realign_reused.data();
+    c.realign_accepted = b->t.realign_accepted.data();
+    c.n_rms = b->t.n_rms;
+    c.n_rms_window = b->t.n_rms_window;
+    c.n_cells = b->t.n_cells;
+    c.fft_nlogn = b->t.fft_nlogn;
+    return &b->c;
+}
+
+int device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// One batch through the engine with per-pair results and status.
+int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
+              const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, visqol_result **out, int32_t *status,
+              visqol_b200_trace **traces) {
+    std::vector<vqb::PairOutcome> res;
+    try {
+        c->engine->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
+    } catch (const Error &e) {
+        for (size_t i = 0; i < n; ++i) {
+            out[i] = nullptr;
+            if (status) status[i] = e.code;
+            if (traces) traces[i] = nullptr;
+        }
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(VISQOL_E_OUT_OF_MEMORY, "OutOfMemory");
+    } catch (const std::exception &e) {
+        return fail(VISQOL_E_INTERNAL, e.what());
+    }
+    int first = VISQOL_OK;
+    for (size_t i = 0; i < n; ++i) {
+        out[i] = nullptr;
+        if (traces) traces[i] = nullptr;
+        int rc = res[i].code;
+        if (rc == VISQOL_OK) {
+            out[i] = box_scores(std::move(res[i].scores));
+            if (traces) traces[i] = box_trace(std::move(res[i].trace));
+        } else {
+            set_error(res[i].message);
+        }
+        if (status) status[i] = rc;
+        if (rc != VISQOL_OK && first == VISQOL_OK) first = rc;
+    }
+    if (first != VISQOL_OK) {
+        for (size_t i = 0; i < n; ++i)
+            if (res[i].code == first) {
+                set_error(res[i].message);
+                break;
+            }
+    }
+    return first;
+}
+
+}  // namespace
+
+void vqb::set_last_error(const std::string &message) { set_error(message); }
+
+extern "C" {
+
+uint32_t visqol_abi_version(void) { return VISQOL_ABI_VERSION; }
+
+const char *visqol_version(void) { return "0.1.0-b200"; }
+
+const char *visqol_last_error(void) { return g_error; }
+
+uint32_t visqol_available_backends(void) { return device_count() > 0 ? (1u << VISQOL_BACKEND_CUDA) : 0u; }
+
+void visqol_options_default(visqol_options *o) {
+    if (!o) return;
+    o->mode = VISQOL_MODE_AUDIO;
+    o->search_window_radius = 60;
+    o->use_unscaled_speech_mos_mapping = 0;
+    o->disable_global_alignment = 0;
+    o->disable_realignment = 0;
+    o->use_lattice_model = 1;
+    o->model_path = nullptr;
+    o->backend = VISQOL_BACKEND_CUDA;
+    o->precision = VISQOL_PRECISION_AUTO;
+}
+
+int visqol_create(const visqol_options *in, visqol_ctx **out) {
+    if (!out) return fail(VISQOL_E_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    visqol_options o;
+    visqol_options_default(&o);
+    if (in) o = *in;
+    if (o.mode > 1) return fail(VISQOL_E_INVALID_ARGUMENT, "invalid mode " + std::to_string(o.mode));
+    if (o.backend > VISQOL_BACKEND_VULKAN) return fail(VISQOL_E_INVALID_ARGUMENT, "invalid backend " + std::to_string(o.backend));
+    if (o.precision > VISQOL_PRECISION_AUTO)
+        return fail(VISQOL_E_INVALID_ARGUMENT, "invalid precision " + std::to_string(o.precision));
+    if (o.backend != VISQOL_BACKEND_CUDA)
+        return fail(VISQOL_E_BACKEND, "BackendUnavailable: this libvisqol serves backend cuda (2) only");
+    if (o.precision == VISQOL_PRECISION_FAST || o.precision == VISQOL_PRECISION_BALANCED)
+        return fail(VISQOL_E_BACKEND, "BackendUnavailable: only the exact (f64) form is built");
+    auto c = std::make_unique<visqol_ctx>();
+    c->opt.speech = o.mode == VISQOL_MODE_SPEECH;
+    c->opt.radius = o.search_window_radius > 0 ? o.search_window_radius : 60;
+    c->opt.unscaled_speech = o.use_unscaled_speech_mos_mapping != 0;
+    c->opt.disable_global_alignment = o.disable_global_alignment != 0;
+    c->opt.disable_realignment = o.disable_realignment != 0;
+    try {
+        if (c->opt.speech && o.use_lattice_model)
+            return fail(VISQOL_E_MODEL, "UnsupportedOp: the TF-Lattice speech mapper is not in this build; "
+                                        "set use_lattice_model = 0 for the exponential mapping");
+        if (!c->opt.speech) {
+            const std::string text = (o.model_path && o.model_path[0]) ? vqb::host::read_file(o.model_path)
+                                                                       : vqb::host::default_svr_text();
+            c->svr = std::make_shared<vqb::host::Svr>(vqb::host::parse_svr(text));
+        }
+        const int ndev = device_count();
+        if (ndev == 0) return fail(VISQOL_E_BACKEND, "BackendUnavailable: no CUDA device");
+        // VISQOL_CUDA_DEVICE picks the GPU (one process per GPU); else device 0.
+        int dev = 0;
+        if (const char *env = std::getenv("VISQOL_CUDA_DEVICE")) dev = std::atoi(env);
+        if (dev < 0 || dev >= ndev) return fail(VISQOL_E_INVALID_ARGUMENT, "VISQOL_CUDA_DEVICE out of range");
+        c->engine = std::make_unique<vqb::Engine>(dev, c->opt, c->svr);
+    } catch (const Error &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(VISQOL_E_OUT_OF_MEMORY, "OutOfMemory");
+    } catch (const std::exception &e) {
+        return fail(VISQOL_E_INTERNAL, e.what());
+    }
+    *out = c.release();
+    return VISQOL_OK;
+}
+
+void visqol_destroy(visqol_ctx *c) { delete c; }
+
+int visqol_measure(visqol_ctx *c, const double *ref, size_t ref_len, const double *deg, size_t deg_len,
+                   uint32_t sample_rate, visqol_result **out) {
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (!out) return fail(VISQOL_E_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if ((!ref && ref_len) || (!deg && deg_len)) return fail(VISQOL_E_INVALID_ARGUMENT, "signal pointer is NULL");
+    int32_t st = 0;
+    return run_batch(c, 1, &ref, &ref_len, &deg, &deg_len, sample_rate, false, out, &st, nullptr);
+}
+
+int visqol_measure_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,
+                         const double *const *degs, const size_t *deg_lens, uint32_t sample_rate, uint32_t num_threads,
+                         visqol_result **out, int32_t *status) {
+    (void)num_threads;
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (n == 0) return VISQOL_OK;
+    if (!out) return fail(VISQOL_E_INVALID_ARGUMENT, "out is NULL");
+    if (!refs) return fail(VISQOL_E_INVALID_ARGUMENT, "refs is NULL");
+    if (!ref_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "ref_lens is NULL");
+    if (!degs) return fail(VISQOL_E_INVALID_ARGUMENT, "degs is NULL");
+    if (!deg_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "deg_lens is NULL");
+    return run_batch(c, n, refs, ref_lens, degs, deg_lens, sample_rate, false, out, status, nullptr);
+}
+
+int visqol_measure_files(visqol_ctx *c, const char *ref_path, const char *deg_path, visqol_result **out) {
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (!out) return fail(VISQOL_E_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (!ref_path) return fail(VISQOL_E_INVALID_ARGUMENT, "ref_path is NULL");
+    if (!deg_path) return fail(VISQOL_E_INVALID_ARGUMENT, "deg_path is NULL");
+    uint32_t rr = 0, dr = 0;
+    std::vector<double> r, d;
+    try {
+        r = vqb::host::decode_wav(vqb::host::read_file(ref_path), &rr);
+    } catch (const Error &e) {
+        return fail(e.code, std::string(ref_path) + ": " + e.what());
+    }
+    try {
+        d = vqb::host::decode_wav(vqb::host::read_file(deg_path), &dr);
+    } catch (const Error &e) {
+        return fail(e.code, std::string(deg_path) + ": " + e.what());
+    }
+    if (rr != dr)
+        return fail(VISQOL_E_SIGNAL, "Input audio signals have different sample rates! Reference audio sample rate: " +
+                                         std::to_string(rr) + ". Degraded audio sample rate: " + std::to_string(dr));
+    const double *rp = r.data(), *dp = d.data();
+    const size_t rl = r.size(), dl = d.size();
+    int32_t st = 0;
+    return run_batch(c, 1, &rp, &rl, &dp, &dl, rr, false, out, &st, nullptr);
+}
+
+int visqol_measure_files_batch(visqol_ctx *c, size_t n, const char *const *ref_paths, const char *const *deg_paths,
+                               uint32_t num_threads, visqol_result **out, int32_t *status) {
+    (void)num_threads;
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (n == 0) return VISQOL_OK;
+    if (!out) return fail(VISQOL_E_INVALID_ARGUMENT, "out is NULL");
+    if (!ref_paths) return fail(VISQOL_E_INVALID_ARGUMENT, "ref_paths is NULL");
+    if (!deg_paths) return fail(VISQOL_E_INVALID_ARGUMENT, "deg_paths is NULL");
+    std::vector<std::vector<double>> r(n), d(n);
+    std::vector<uint32_t> rate(n, 0);
+    std::vector<int32_t> codes(n, VISQOL_OK);
+    for (size_t i = 0; i < n; ++i) {
+        out[i] = nullptr;
+        uint32_t rr = 0, dr = 0;
+        try {
+            r[i] = vqb::host::decode_wav(vqb::host::read_file(ref_paths[i]), &rr);
+        } catch (const Error &e) {
+            codes[i] = fail(e.code, std::string(ref_paths[i]) + ": " + e.what());
+            continue;
+        }
+        try {
+            d[i] = vqb::host::decode_wav(vqb::host::read_file(deg_paths[i]), &dr);
+        } catch (const Error &e) {
+            codes[i] = fail(e.code, std::string(deg_paths[i]) + ": " + e.what());
+            continue;
+        }
+        rate[i] = rr;
+        if (rr != dr) {
+            codes[i] = fail(VISQOL_E_SIGNAL, "pair " + std::to_string(i) + ": reference and degraded sample rates differ (" +
+                                                 std::to_string(rr) + " vs " + std::to_string(dr) + ")");
+        }
+    }
+    std::map<uint32_t, std::vector<size_t>> groups;
+    for (size_t i = 0; i < n; ++i)
+        if (codes[i] == VISQOL_OK) groups[rate[i]].push_back(i);
+    for (auto &g : groups) {
+        const size_t m = g.second.size();
+        std::vector<const double *> rp(m), dp(m);
+        std::vector<size_t> rl(m), dl(m);
+        for (size_t k = 0; k < m; ++k) {
+            const size_t i = g.second[k];
+            rp[k] = r[i].data(), dp[k] = d[i].data(), rl[k] = r[i].size(), dl[k] = d[i].size();
+        }
+        std::vector<visqol_result *> res(m, nullptr);
+        std::vector<int32_t> st(m, 0);
+        run_batch(c, m, rp.data(), rl.data(), dp.data(), dl.data(), g.first, false, res.data(), st.data(), nullptr);
+        for (size_t k = 0; k < m; ++k) {
+            out[g.second[k]] = res[k];
+            codes[g.second[k]] = st[k];
+        }
+    }
+    int first = VISQOL_OK;
+    for (size_t i = 0; i < n; ++i) {
+        if (status) status[i] = codes[i];
+        if (codes[i] != VISQOL_OK && first == VISQOL_OK) first = codes[i];
+    }
+    return first;
+}
+
+void visqol_result_free(visqol_result *r) {
+    if (!r) return;
+    delete reinterpret_cast<Box *>(r);
+}
+
+int visqol_b200_measure_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,
+                              const double *const *degs, const size_t *deg_lens, uint32_t sample_rate, uint32_t flags,
+                              visqol_result **out, int32_t *status, visqol_b200_trace **traces) {
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (n == 0) return VISQOL_OK;
+    if (!out || !refs || !ref_lens || !degs || !deg_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    return run_batch(c, n, refs, ref_lens, degs, deg_lens, sample_rate, (flags & VISQOL_B200_DEVICE_INPUTS) != 0, out,
+                     status, traces);
+}
+
+void visqol_b200_trace_free(visqol_b200_trace *t) {
+    if (!t) return;
+    delete reinterpret_cast<TraceBox *>(t);
+}
+
+int visqol_b200_last_timing(visqol_ctx *c, visqol_b200_timing *out) {
+    if (!c || !out) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    const vqb::Timing &t = c->engine->last_timing();
+    out->total_ms = t.total_ms;
+    out->lag_ms = t.lag_ms;
+    out->spectrogram_ms = t.spectrogram_ms;
+    out->prep_ms = t.prep_ms;
+    out->nsim_ms = t.nsim_ms;
+    out->realign_ms = t.realign_ms;
+    out->gammatone_kernel_ms = t.gammatone_kernel_ms;
+    out->gammatone_launches = t.gammatone_launches;
+    out->gammatone_rms = t.gammatone_rms;
+    out->gammatone_window = t.gammatone_window;
+    out->kernel_launches = t.kernel_launches;
+    out->h2d_bytes = t.h2d_bytes;
+    out->d2h_bytes = t.d2h_bytes;
+    out->host_syncs = t.host_syncs;
+    return VISQOL_OK;
+}
+
+int visqol_b200_device_info(int device, char *name, size_t name_len, int *sm_count, int *cc_major, int *cc_minor) {
+    if (device_count() <= device) return fail(VISQOL_E_BACKEND, "no such CUDA device");
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return fail(VISQOL_E_BACKEND, "cudaGetDeviceProperties failed");
+    if (name && name_len) std::snprintf(name, name_len, "%s", p.name);
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    if (cc_major) *cc_major = p.major;
+    if (cc_minor) *cc_minor = p.minor;
+    return VISQOL_OK;
+}
+
+}  // extern "C"

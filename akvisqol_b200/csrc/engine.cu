@@ -1,0 +1,786 @@
+// Batched ViSQOL pipeline on one GPU (exact f64 form).
+//
+// The reference's CPU model runs a pair's stages in sequence
+// (src/visqol.zig:394-487); its data-dependent steps (frame counts follow the
+// global lag, patch windows follow the frame counts, realignment slices
+// follow the DP matches, trimmed lengths follow the per-patch lags) are
+// planned here on the host between device phases, for all pairs of the batch
+// at once, so every kernel launch covers the whole batch:
+//
+//   1. envelopes + FFT lag search, SPL energies        -> lags, energies
+//   2. (host) SPL factors, frames, patches, search windows
+//   3. aligned+scaled signals, gammatone spectrograms, dB/floors, NSIM
+//      table, DP, per-match band statistics            -> matches
+//   4. (host) realignment slices
+//   5. slice envelopes + FFT lag search                 -> per-patch lags
+//   6. (host) trimmed geometry, grid-frame reuse
+//   7. realigned spectrograms, dB/floors, band statistics
+//   8. (host) accept rule, pooled features, MOS
+//
+// Signals and intermediate spectrograms stay in HBM; only lags, energies,
+// matches and statistics cross to the host.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kernels.h"
+
+namespace vqb {
+
+void cuda_check(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation) throw Error(kOom, std::string(what) + ": " + cudaGetErrorString(e));
+    throw Error(kBackend, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Arenas
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kAlign = 256;
+constexpr size_t kChunk = size_t(256) << 20;
+inline size_t round_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+}  // namespace
+
+Arena::~Arena() {
+    for (auto &c : chunks_) cudaFree(c.base);
+}
+void Arena::reset() {
+    for (auto &c : chunks_) c.used = 0;
+    current_ = 0;
+}
+void *Arena::alloc(size_t bytes) {
+    bytes = round_up(bytes ? bytes : 1);
+    while (current_ < chunks_.size()) {
+        Chunk &c = chunks_[current_];
+        if (c.used + bytes <= c.size) {
+            void *p = c.base + c.used;
+            c.used += bytes;
+            return p;
+        }
+        ++current_;
+    }
+    Chunk c{nullptr, std::max(bytes, kChunk), 0};
+    VQB_CUDA(cudaMalloc(&c.base, c.size));
+    c.used = bytes;
+    chunks_.push_back(c);
+    current_ = chunks_.size() - 1;
+    return c.base;
+}
+size_t Arena::reserved() const {
+    size_t s = 0;
+    for (auto &c : chunks_) s += c.size;
+    return s;
+}
+
+PinnedArena::~PinnedArena() {
+    for (auto &c : chunks_) cudaFreeHost(c.base);
+}
+void PinnedArena::reset() {
+    for (auto &c : chunks_) c.used = 0;
+    current_ = 0;
+}
+void *PinnedArena::alloc(size_t bytes) {
+    bytes = round_up(bytes ? bytes : 1);
+    while (current_ < chunks_.size()) {
+        Chunk &c = chunks_[current_];
+        if (c.used + bytes <= c.size) {
+            void *p = c.base + c.used;
+            c.used += bytes;
+            return p;
+        }
+        ++current_;
+    }
+    Chunk c{nullptr, std::max(bytes, size_t(64) << 20), 0};
+    VQB_CUDA(cudaMallocHost(&c.base, c.size));
+    c.used = bytes;
+    chunks_.push_back(c);
+    current_ = chunks_.size() - 1;
+    return c.base;
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr)
+    : device_(device), opt_(opt), svr_(std::move(svr)) {
+    nb_ = opt.speech ? 21 : 32;
+    patch_ = opt.speech ? 20 : 30;
+    max_freq_ = opt.speech ? 8000.0 : -1.0;
+    VQB_CUDA(cudaSetDevice(device_));
+    VQB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    events_.resize(8);
+    for (auto &e : events_) VQB_CUDA(cudaEventCreate(&e));
+    for (auto &e : gt_events_) VQB_CUDA(cudaEventCreate(&e));
+    fft_init_attributes();
+    nsim_init_attributes();
+    VQB_CUDA(cudaGetLastError());
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto &kv : rates_) {
+        cudaFree(kv.second.d_coeffs);
+        cudaFree(kv.second.d_hann);
+    }
+    for (auto &kv : twiddles_) cudaFree(kv.second);
+    for (auto e : events_) cudaEventDestroy(e);
+    for (auto e : gt_events_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+const Engine::RateCache &Engine::rate_cache(uint32_t sr) {
+    auto it = rates_.find(sr);
+    if (it != rates_.end()) return it->second;
+    RateCache rc;
+    rc.fb = host::make_filterbank(nb_, sr, 50.0, max_freq_ > 0 ? max_freq_ : (double)sr / 2.0);
+    rc.geo = host::analysis_geometry(sr);
+    const std::vector<double> w = host::hann(rc.geo.window);
+    VQB_CUDA(cudaMalloc(&rc.d_coeffs, nb_ * sizeof(BandCoeffs)));
+    VQB_CUDA(cudaMalloc(&rc.d_hann, std::max<size_t>(1, w.size()) * sizeof(double)));
+    VQB_CUDA(cudaMemcpy(rc.d_coeffs, rc.fb.run.data(), nb_ * sizeof(BandCoeffs), cudaMemcpyHostToDevice));
+    if (!w.empty()) VQB_CUDA(cudaMemcpy(rc.d_hann, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return rates_.emplace(sr, std::move(rc)).first->second;
+}
+
+const double2 *Engine::twiddles(size_t n) {
+    auto it = twiddles_.find(n);
+    if (it != twiddles_.end()) return it->second;
+    const std::vector<double2> t = host::twiddles(n);
+    double2 *d = nullptr;
+    VQB_CUDA(cudaMalloc(&d, std::max<size_t>(1, t.size()) * sizeof(double2)));
+    if (!t.empty()) VQB_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    twiddles_[n] = d;
+    return d;
+}
+
+template <class T>
+T *Engine::upload(const std::vector<T> &v) {
+    return static_cast<T *>(upload_bytes(v.data(), v.size() * sizeof(T)));
+}
+
+void *Engine::upload_bytes(const void *src, size_t bytes) {
+    void *h = pinned_.alloc(bytes);
+    if (bytes) std::memcpy(h, src, bytes);
+    void *d = arena_.alloc(bytes);
+    if (bytes) VQB_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_));
+    timing_.h2d_bytes += bytes;
+    return d;
+}
+
+void Engine::d2h(void *dst, const void *src, size_t bytes) {
+    if (!bytes) return;
+    VQB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
+    timing_.d2h_bytes += bytes;
+}
+
+void Engine::sync() {
+    VQB_CUDA(cudaGetLastError());
+    VQB_CUDA(cudaStreamSynchronize(stream_));
+    ++timing_.host_syncs;
+}
+
+void Engine::record(cudaEvent_t e) { VQB_CUDA(cudaEventRecord(e, stream_)); }
+
+float Engine::elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    VQB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
+    if (jobs.empty()) return;
+    // Group by FFT size; bound each submission's buffer.
+    std::map<int64_t, std::vector<size_t>> groups;
+    for (size_t i = 0; i < jobs.size(); ++i) groups[jobs[i].n].push_back(i);
+    const size_t budget = size_t(4) << 30;
+    for (auto &g : groups) {
+        const int64_t n = g.first;
+        const double2 *top = twiddles((size_t)n);
+        const size_t per = std::max<size_t>(1, budget / ((size_t)n * sizeof(double2)));
+        for (size_t c0 = 0; c0 < g.second.size(); c0 += per) {
+            const size_t cnt = std::min(per, g.second.size() - c0);
+            double2 *z = arena_.alloc_n<double2>((size_t)n * cnt);
+            std::vector<LagJob> chunk(cnt);
+            for (size_t k = 0; k < cnt; ++k) {
+                chunk[k] = jobs[g.second[c0 + k]];
+                chunk[k].z = z + (int64_t)k * n;
+            }
+            LagJob *d_jobs = upload(chunk);
+            const int parts = argmax_parts(n);
+            double *pv = arena_.alloc_n<double>((size_t)parts * cnt);
+            int64_t *pk = arena_.alloc_n<int64_t>((size_t)parts * cnt);
+            launch_pack(d_jobs, (int)cnt, n, raw, stream_);
+            launch_fft(z, n, false, top, (int)cnt, n, stream_);
+            launch_cross(z, n, (int)cnt, n, stream_);
+            launch_fft(z, n, true, top, (int)cnt, n, stream_);
+            launch_argmax(z, d_jobs, (int)cnt, n, n, pv, pk, stream_);
+        }
+    }
+}
+
+void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags) {
+    arena_.reset();
+    pinned_.reset();
+    std::vector<LagJob> jobs(njobs);
+    int64_t *d_lags = arena_.alloc_n<int64_t>(njobs);
+    double *d_stats = arena_.alloc_n<double>(8 * njobs);
+    std::vector<SumJob> sums;
+    for (size_t i = 0; i < njobs; ++i) {
+        LagJob &j = jobs[i];
+        j.a = a[i];
+        j.b = b[i];
+        j.biggest = std::max(a[i].len, b[i].len);
+        j.n = (int64_t)host::fft_size_for((size_t)j.biggest);
+        j.stats_a = d_stats + 8 * i;
+        j.stats_b = d_stats + 8 * i + 4;
+        j.lag_out = d_lags + i;
+        sums.push_back(SumJob{a[i], j.stats_a});
+        sums.push_back(SumJob{b[i], j.stats_b});
+    }
+    VQB_CUDA(cudaMemsetAsync(d_lags, 0, njobs * sizeof(int64_t), stream_));
+    std::vector<size_t> empty;
+    std::vector<LagJob> run;
+    std::vector<size_t> where;
+    for (size_t i = 0; i < njobs; ++i)
+        if (jobs[i].biggest > 0) run.push_back(jobs[i]), where.push_back(i);
+    if (!raw && !sums.empty()) launch_envelope_stats(upload(sums), (int)sums.size(), stream_);
+    launch_lag_jobs(run, raw);
+    int64_t *h = pinned_.alloc_n<int64_t>(njobs);
+    d2h(h, d_lags, njobs * sizeof(int64_t));
+    sync();
+    std::memcpy(h_lags, h, njobs * sizeof(int64_t));
+}
+
+void Engine::spectrogram(const host::Filterbank &fb, const double *d_hann, size_t window, size_t hop,
+                         const double *d_x, size_t len, double *d_out, size_t nf) {
+    arena_.reset();
+    pinned_.reset();
+    if (nf == 0) return;
+    BandCoeffs *d_coeffs = upload(fb.run);
+    SpecJob job{VSig{d_x, 0, (int64_t)len, (int64_t)len}, (int64_t)nf, d_out};
+    SpecJob *d_job = upload(std::vector<SpecJob>{job});
+    const int nbi = (int)fb.nb;
+    const int F = gammatone_frames_per_cta(nbi);
+    const size_t tsz = gammatone_tile_size();
+    std::vector<char> tiles;
+    int ntiles = 0;
+    for (size_t f = 0; f < nf; f += F, ++ntiles) {
+        tiles.resize(tiles.size() + tsz);
+        fill_gammatone_tile(tiles.data() + tiles.size() - tsz, 0, (int)f);
+    }
+    void *d_tiles = upload_bytes(tiles.data(), tiles.size());
+    launch_gammatone(d_job, d_tiles, ntiles, d_coeffs, nbi, d_hann, (int)window, (int)hop, stream_);
+    sync();
+}
+
+namespace {
+
+struct RealignPatch {
+    size_t mi;
+    host::Slice rl, dl;
+    int64_t rlen, dlen;
+    int64_t lag = 0;
+    host::Trim trim{};
+    size_t nf = 0;
+    double *stats = nullptr;  // 8: slice envelope stats
+    double *rs_raw = nullptr, *ds_raw = nullptr, *rs = nullptr, *ds = nullptr, *st = nullptr;
+    uint8_t reused = 0;
+};
+
+struct PairState {
+    bool live = true;
+    int code = 0;
+    std::string msg;
+    const double *ref = nullptr, *deg = nullptr;  // device
+    const double *h_ref = nullptr;                // host (VAD)
+    size_t rl = 0, dl = 0;
+    bool lag_job = false;
+    double *stats = nullptr;  // device: ref[4], deg[4], aligned energy, aligned length
+    host::Aligned al{};
+    double factor = 1.0;
+    size_t nf_ref = 0, nf_deg = 0;
+    std::vector<int64_t> idx;
+    host::Search search;
+    size_t width = 0;
+    double *deg_al = nullptr, *ref_raw = nullptr, *deg_raw = nullptr, *ref_prep = nullptr, *deg_prep = nullptr;
+    double *pad = nullptr, *mu = nullptr, *dms = nullptr, *sds = nullptr, *terms = nullptr, *sims = nullptr;
+    double *dp = nullptr;
+    int64_t *bt = nullptr, *offs = nullptr;
+    uint8_t *valid = nullptr;
+    double *mstats = nullptr;
+    std::vector<host::Match> matches;
+    std::vector<RealignPatch> rps;
+    PairTrace trace;
+    void fail(int c, const std::string &m) {
+        live = false;
+        code = c;
+        msg = m;
+    }
+};
+
+}  // namespace
+
+void Engine::measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
+                           const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
+                           std::vector<PairOutcome> &out) {
+    out.assign(n, PairOutcome{});
+    timing_ = Timing{};
+    if (n == 0) return;
+    VQB_CUDA(cudaSetDevice(device_));
+    if (sample_rate == 0) {
+        for (auto &o : out) o.code = kInvalid, o.message = "InvalidInput";
+        return;
+    }
+    arena_.reset();
+    pinned_.reset();
+    const RateCache &rc = rate_cache(sample_rate);
+    const size_t W = rc.geo.window, H = rc.geo.hop, NB = nb_, P = patch_;
+    const double fd = rc.geo.frame_duration;
+    const int nbi = (int)NB;
+    std::vector<PairState> ps(n);
+    const uint64_t launches0 = launch_counter();
+    record(events_[0]);
+
+    // ---- inputs -----------------------------------------------------------
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        s.rl = ref_lens[i];
+        s.dl = deg_lens[i];
+        if ((s.rl && !refs[i]) || (s.dl && !degs[i])) {
+            s.fail(kInvalid, "signal pointer is NULL");
+            continue;
+        }
+        if (device_inputs) {
+            s.ref = refs[i];
+            s.deg = degs[i];
+        } else {
+            double *r = arena_.alloc_n<double>(s.rl), *d = arena_.alloc_n<double>(s.dl);
+            if (s.rl) VQB_CUDA(cudaMemcpyAsync(r, refs[i], s.rl * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            if (s.dl) VQB_CUDA(cudaMemcpyAsync(d, degs[i], s.dl * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            timing_.h2d_bytes += (s.rl + s.dl) * sizeof(double);
+            s.ref = r;
+            s.deg = d;
+            s.h_ref = refs[i];
+        }
+        s.stats = arena_.alloc_n<double>(10);
+    }
+
+    // ---- 1: global lag and SPL energies --------------------------------
+    int64_t *d_lags = arena_.alloc_n<int64_t>(n);
+    VQB_CUDA(cudaMemsetAsync(d_lags, 0, n * sizeof(int64_t), stream_));
+    {
+        std::vector<SumJob> sums;
+        std::vector<LagJob> lag_jobs;
+        for (size_t i = 0; i < n; ++i) {
+            PairState &s = ps[i];
+            if (!s.live) continue;
+            const VSig r{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, d{s.deg, 0, (int64_t)s.dl, (int64_t)s.dl};
+            sums.push_back(SumJob{r, s.stats});
+            if (!opt_.disable_global_alignment && s.rl > 0 && s.dl > 0) {
+                s.lag_job = true;
+                sums.push_back(SumJob{d, s.stats + 4});
+                LagJob j{};
+                j.a = r;
+                j.b = d;
+                j.biggest = (int64_t)std::max(s.rl, s.dl);
+                j.n = (int64_t)host::fft_size_for((size_t)j.biggest);
+                j.stats_a = s.stats;
+                j.stats_b = s.stats + 4;
+                j.lag_out = d_lags + i;
+                lag_jobs.push_back(j);
+                s.trace.fft_nlogn += 2.0 * (double)j.n * std::log2((double)j.n);
+            }
+        }
+        if (!sums.empty()) launch_envelope_stats(upload(sums), (int)sums.size(), stream_);
+        launch_lag_jobs(lag_jobs, false);
+        std::vector<char> args;
+        const size_t asz = aligned_energy_args_size();
+        int na = 0;
+        for (size_t i = 0; i < n; ++i) {
+            PairState &s = ps[i];
+            if (!s.live) continue;
+            args.resize(args.size() + asz);
+            fill_aligned_energy_args(args.data() + args.size() - asz, VSig{s.deg, 0, (int64_t)s.dl, (int64_t)s.dl},
+                                     (int64_t)s.rl, d_lags + i, s.stats + 8);
+            ++na;
+        }
+        if (na) launch_aligned_energy(upload_bytes(args.data(), args.size()), na, stream_);
+    }
+    int64_t *h_lags = pinned_.alloc_n<int64_t>(n);
+    double *h_stats = pinned_.alloc_n<double>(10 * n);
+    d2h(h_lags, d_lags, n * sizeof(int64_t));
+    for (size_t i = 0; i < n; ++i)
+        if (ps[i].live) d2h(h_stats + 10 * i, ps[i].stats, 10 * sizeof(double));
+    record(events_[1]);
+    sync();
+
+    // ---- 2: plan frames, patches and search windows (host) --------------
+    std::vector<SpecJob> spec_jobs;
+    std::vector<char> scale_args;
+    int nscale = 0;
+    int64_t max_al = 0;
+    std::vector<PrepJob> prep_jobs;
+    std::vector<PlaneJob> plane_jobs;
+    std::vector<RefTermsJob> term_jobs;
+    std::vector<TableTask> tasks;
+    std::vector<DpJob> dp_jobs;
+    std::vector<StatsJob> stat_jobs;
+    int max_width = 0;
+    const int per_cta = table_offsets_per_cta();
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.live) continue;
+        try {
+            const int64_t lag = s.lag_job ? h_lags[i] : 0;
+            s.trace.global_lag = lag;
+            s.al = opt_.disable_global_alignment ? host::Aligned{0, 0, (int64_t)s.dl, 0.0}
+                                                 : host::apply_lag_geometry(s.rl, s.dl, lag, sample_rate);
+            const double *st = h_stats + 10 * i;
+            s.factor = host::spl_factor(st[2], s.rl, st[8], (size_t)s.al.len);
+            s.trace.spl_factor = s.factor;
+            s.trace.deg_len = (uint64_t)s.al.len;
+            if (s.rl <= W || (size_t)s.al.len <= W) throw Error(kSignal, "SpectrogramTooShort");
+            s.nf_ref = host::num_frames(s.rl, W, H);
+            s.nf_deg = host::num_frames((size_t)s.al.len, W, H);
+            s.trace.nf_ref = s.nf_ref;
+            s.trace.nf_deg = s.nf_deg;
+            if (opt_.speech) {
+                std::vector<double> tmp;
+                const double *hr = s.h_ref;
+                if (!hr) {
+                    tmp.resize(s.rl);
+                    VQB_CUDA(cudaMemcpy(tmp.data(), s.ref, s.rl * sizeof(double), cudaMemcpyDeviceToHost));
+                    hr = tmp.data();
+                }
+                s.idx = host::vad_patch_indices(hr, s.rl, s.nf_ref, P, W, 0.25);
+            } else {
+                s.idx = host::ref_patch_indices(s.nf_ref, P);
+            }
+            if (s.idx.empty()) throw Error(kSignal, "NoPatches");
+            s.search = host::plan_search(s.idx, s.nf_ref, s.nf_deg, P, opt_.radius);
+        } catch (const Error &e) {
+            s.fail(e.code, e.what());
+            continue;
+        }
+        const size_t np = s.search.np;
+        s.width = s.nf_deg;
+        for (size_t p = 0; p < np; ++p) s.width = std::max(s.width, (size_t)s.search.hi[p] + P);
+        max_width = std::max(max_width, (int)s.width);
+        s.deg_al = arena_.alloc_n<double>((size_t)s.al.len);
+        s.ref_raw = arena_.alloc_n<double>(NB * s.nf_ref);
+        s.deg_raw = arena_.alloc_n<double>(NB * s.nf_deg);
+        s.ref_prep = arena_.alloc_n<double>(NB * s.nf_ref);
+        s.deg_prep = arena_.alloc_n<double>(NB * s.nf_deg);
+        const size_t plane = NB * s.width;
+        s.pad = arena_.alloc_n<double>(4 * plane);
+        s.mu = s.pad + plane;
+        s.dms = s.mu + plane;
+        s.sds = s.dms + plane;
+        s.terms = arena_.alloc_n<double>(np * 4 * NB * P);
+        s.sims = arena_.alloc_n<double>(np * s.nf_deg);
+        s.dp = arena_.alloc_n<double>(np * s.nf_deg);
+        s.bt = arena_.alloc_n<int64_t>(np * s.nf_deg);
+        s.offs = arena_.alloc_n<int64_t>(np);
+        s.valid = arena_.alloc_n<uint8_t>(np);
+        s.mstats = arena_.alloc_n<double>(np * (3 * NB + 1));
+        // aligned[i] = deg[i - lead + skip] (applyLag), scaled (scaleToMatchSpl)
+        const VSig src{s.deg + s.al.skip, s.al.lead, (int64_t)s.dl - s.al.skip, s.al.len};
+        scale_args.resize(scale_args.size() + scale_args_size());
+        fill_scale_args(scale_args.data() + scale_args.size() - scale_args_size(), src, s.factor, s.deg_al);
+        ++nscale;
+        max_al = std::max(max_al, s.al.len);
+        spec_jobs.push_back(SpecJob{VSig{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, (int64_t)s.nf_ref, s.ref_raw});
+        spec_jobs.push_back(SpecJob{VSig{s.deg_al, 0, s.al.len, s.al.len}, (int64_t)s.nf_deg, s.deg_raw});
+        s.trace.n_rms += NB * (s.nf_ref + s.nf_deg);
+        prep_jobs.push_back(PrepJob{s.ref_raw, s.deg_raw, s.ref_prep, s.deg_prep, (int32_t)s.nf_ref, (int32_t)s.nf_deg});
+        plane_jobs.push_back(PlaneJob{s.deg_prep, (int32_t)s.nf_deg, (int32_t)s.width, s.pad, s.mu, s.dms, s.sds});
+        int64_t *d_lo = nullptr;
+        {
+            std::vector<int64_t> lohi(2 * np);
+            std::copy(s.search.lo.begin(), s.search.lo.end(), lohi.begin());
+            std::copy(s.search.hi.begin(), s.search.hi.end(), lohi.begin() + np);
+            d_lo = upload(lohi);
+        }
+        for (size_t p = 0; p < np; ++p) {
+            double *terms = s.terms + p * 4 * NB * P;
+            term_jobs.push_back(RefTermsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], terms});
+            for (int64_t off0 = s.search.lo[p]; off0 <= s.search.hi[p]; off0 += per_cta)
+                tasks.push_back(TableTask{terms, s.pad, s.mu, s.dms, s.sds, (int32_t)s.width, (int32_t)off0,
+                                          (int32_t)s.search.hi[p], s.sims + p * s.nf_deg});
+            s.trace.n_cells += (uint64_t)(s.search.hi[p] - s.search.lo[p] + 1) * NB * P;
+            double *ms = s.mstats + p * (3 * NB + 1);
+            stat_jobs.push_back(StatsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], s.deg_prep,
+                                         (int32_t)s.nf_deg, 0, (int32_t)s.nf_deg, (int32_t)P, s.offs + p,
+                                         s.valid + p, ms, ms + NB, ms + 2 * NB, ms + 3 * NB});
+            s.trace.n_cells += NB * P;
+        }
+        dp_jobs.push_back(DpJob{s.sims, d_lo, d_lo + np, (int32_t)np, (int64_t)s.nf_deg, s.dp, s.bt, s.offs, s.valid});
+    }
+
+    // ---- 3: spectrograms, prep, NSIM table, DP, match statistics ----------
+    auto run_gammatone = [&](const std::vector<SpecJob> &jobs) {
+        if (jobs.empty()) return;
+        SpecJob *d_jobs = upload(jobs);
+        const int F = gammatone_frames_per_cta(nbi);
+        const size_t tsz = gammatone_tile_size();
+        std::vector<char> tiles;
+        int ntiles = 0;
+        uint64_t rms = 0;
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            rms += (uint64_t)jobs[j].nf * NB;
+            for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
+                tiles.resize(tiles.size() + tsz);
+                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+            }
+        }
+        void *d_tiles = upload_bytes(tiles.data(), tiles.size());
+        const size_t slot = 2 * timing_.gammatone_launches;
+        record(gt_events_[slot]);
+        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, stream_);
+        record(gt_events_[slot + 1]);
+        timing_.gammatone_launches += 1;
+        timing_.gammatone_rms += rms;
+        timing_.gammatone_window = W;
+    };
+    if (nscale) launch_scale(upload_bytes(scale_args.data(), scale_args.size()), nscale, max_al, stream_);
+    record(events_[2]);
+    run_gammatone(spec_jobs);
+    record(events_[3]);
+    if (!prep_jobs.empty()) launch_prep(upload(prep_jobs), (int)prep_jobs.size(), nbi, stream_);
+    record(events_[4]);
+    if (!plane_jobs.empty()) launch_plane(upload(plane_jobs), (int)plane_jobs.size(), nbi, max_width, stream_);
+    if (!term_jobs.empty()) launch_ref_terms(upload(term_jobs), (int)term_jobs.size(), nbi, (int)P, stream_);
+    if (!tasks.empty()) launch_table(upload(tasks), (int)tasks.size(), nbi, (int)P, stream_);
+    if (!dp_jobs.empty()) launch_dp(upload(dp_jobs), (int)dp_jobs.size(), stream_);
+    if (!stat_jobs.empty()) launch_stats(upload(stat_jobs), (int)stat_jobs.size(), nbi, stream_);
+    std::vector<int64_t *> h_offs(n, nullptr);
+    std::vector<uint8_t *> h_valid(n, nullptr);
+    std::vector<double *> h_ms(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.live) continue;
+        const size_t np = s.search.np;
+        h_offs[i] = pinned_.alloc_n<int64_t>(np);
+        h_valid[i] = pinned_.alloc_n<uint8_t>(np);
+        h_ms[i] = pinned_.alloc_n<double>(np * (3 * NB + 1));
+        d2h(h_offs[i], s.offs, np * sizeof(int64_t));
+        d2h(h_valid[i], s.valid, np);
+        d2h(h_ms[i], s.mstats, np * (3 * NB + 1) * sizeof(double));
+    }
+    record(events_[5]);
+    sync();
+
+    // ---- 4: matches and realignment slices (host) ----------------------
+    const double patch_dur = fd * (double)P;
+    std::vector<SumJob> slice_sums;
+    std::vector<LagJob> slice_lags;
+    int64_t *d_slice_lags = nullptr;
+    size_t n_slices = 0;
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.live) continue;
+        const size_t np = s.search.np;
+        s.matches.resize(np);
+        for (size_t p = 0; p < np; ++p) {
+            host::Match &m = s.matches[p];
+            const double *ms = h_ms[i] + p * (3 * NB + 1);
+            m.means.assign(ms, ms + NB);
+            m.stddevs.assign(ms + NB, ms + 2 * NB);
+            m.energy.assign(ms + 2 * NB, ms + 3 * NB);
+            m.similarity = ms[3 * NB];
+            const int64_t off = h_offs[i][p];
+            if (off >= 0) {
+                m.valid = h_valid[i][p] != 0;
+                if (m.valid) {
+                    m.deg_start = (double)off * fd;
+                    m.deg_end = m.deg_start + patch_dur;
+                }
+                m.ref_start = (double)s.idx[p] * fd;
+                m.ref_end = m.ref_start + patch_dur;
+            }
+            s.trace.ref_index.push_back(s.idx[p]);
+            s.trace.deg_offset.push_back(off);
+            s.trace.valid.push_back(m.valid ? 1 : 0);
+            s.trace.realign_lag.push_back(0);
+            s.trace.realign_frames.push_back(-1);
+            s.trace.realign_reused.push_back(0);
+            s.trace.realign_accepted.push_back(0);
+        }
+        if (opt_.disable_realignment) continue;
+        for (size_t p = 0; p < np; ++p) {
+            const host::Match &m = s.matches[p];
+            if (!m.valid) continue;
+            RealignPatch rp;
+            rp.mi = p;
+            rp.rl = host::slice_layout(s.rl, sample_rate, m.ref_start, m.ref_end);
+            rp.dl = host::slice_layout((size_t)s.al.len, sample_rate, m.deg_start, m.deg_end);
+            rp.rlen = rp.rl.pad + rp.rl.len;
+            rp.dlen = rp.dl.pad + rp.dl.len;
+            if (rp.rlen < (int64_t)W || rp.dlen < (int64_t)W) continue;
+            s.rps.push_back(rp);
+            ++n_slices;
+        }
+    }
+    if (n_slices) {
+        d_slice_lags = arena_.alloc_n<int64_t>(n_slices);
+        double *d_sst = arena_.alloc_n<double>(8 * n_slices);
+        size_t k = 0;
+        for (auto &s : ps) {
+            if (!s.live) continue;
+            for (auto &rp : s.rps) {
+                rp.stats = d_sst + 8 * k;
+                const VSig a{s.ref + rp.rl.base, rp.rl.pad, rp.rl.len, rp.rlen};
+                const VSig b{s.deg_al + rp.dl.base, rp.dl.pad, rp.dl.len, rp.dlen};
+                slice_sums.push_back(SumJob{a, rp.stats});
+                slice_sums.push_back(SumJob{b, rp.stats + 4});
+                LagJob j{};
+                j.a = a;
+                j.b = b;
+                j.biggest = std::max(rp.rlen, rp.dlen);
+                j.n = (int64_t)host::fft_size_for((size_t)j.biggest);
+                j.stats_a = rp.stats;
+                j.stats_b = rp.stats + 4;
+                j.lag_out = d_slice_lags + k;
+                slice_lags.push_back(j);
+                s.trace.fft_nlogn += 2.0 * (double)j.n * std::log2((double)j.n);
+                ++k;
+            }
+        }
+        // ---- 5: slice lags --------------------------------------------------
+        launch_envelope_stats(upload(slice_sums), (int)slice_sums.size(), stream_);
+        launch_lag_jobs(slice_lags, false);
+        int64_t *h_sl = pinned_.alloc_n<int64_t>(n_slices);
+        d2h(h_sl, d_slice_lags, n_slices * sizeof(int64_t));
+        sync();
+
+        // ---- 6: trimmed geometry, frame reuse (host) -------------------------
+        std::vector<SpecJob> rjobs;
+        std::vector<CopyJob> copies;
+        std::vector<PrepJob> rprep;
+        std::vector<StatsJob> rstats;
+        int max_cols = 0;
+        k = 0;
+        for (auto &s : ps) {
+            if (!s.live) continue;
+            for (auto &rp : s.rps) {
+                rp.lag = h_sl[k++];
+                s.trace.realign_lag[rp.mi] = rp.lag;
+                rp.trim = host::trim_geometry(rp.rlen, rp.dlen, rp.lag, sample_rate);
+                rp.nf = host::num_frames((size_t)rp.trim.len, W, H);
+                s.trace.realign_frames[rp.mi] = (int64_t)rp.nf;
+                if (rp.nf == 0) continue;
+                max_cols = std::max(max_cols, (int)rp.nf);
+                rp.rs_raw = arena_.alloc_n<double>(NB * rp.nf);
+                rp.ds_raw = arena_.alloc_n<double>(NB * rp.nf);
+                rp.rs = arena_.alloc_n<double>(NB * rp.nf);
+                rp.ds = arena_.alloc_n<double>(NB * rp.nf);
+                rp.st = arena_.alloc_n<double>(3 * NB + 1);
+                const int64_t g_ref = host::reuse_frame(rp.rl, rp.trim.ref_off, H, rp.nf, s.nf_ref);
+                if (g_ref >= 0) {
+                    copies.push_back(CopyJob{s.ref_raw, (int32_t)s.nf_ref, (int32_t)g_ref, rp.rs_raw, (int32_t)rp.nf});
+                    rp.reused |= 1;
+                } else {
+                    rjobs.push_back(SpecJob{VSig{s.ref + rp.rl.base, rp.rl.pad - rp.trim.ref_off, rp.rl.len, rp.trim.len},
+                                            (int64_t)rp.nf, rp.rs_raw});
+                    s.trace.n_rms += NB * rp.nf;
+                }
+                const int64_t g_deg = host::reuse_frame(rp.dl, rp.trim.deg_off, H, rp.nf, s.nf_deg);
+                if (g_deg >= 0) {
+                    copies.push_back(CopyJob{s.deg_raw, (int32_t)s.nf_deg, (int32_t)g_deg, rp.ds_raw, (int32_t)rp.nf});
+                    rp.reused |= 2;
+                } else {
+                    rjobs.push_back(SpecJob{VSig{s.deg_al + rp.dl.base, rp.dl.pad - rp.trim.deg_off, rp.dl.len, rp.trim.len},
+                                            (int64_t)rp.nf, rp.ds_raw});
+                    s.trace.n_rms += NB * rp.nf;
+                }
+                s.trace.realign_reused[rp.mi] = rp.reused;
+                rprep.push_back(PrepJob{rp.rs_raw, rp.ds_raw, rp.rs, rp.ds, (int32_t)rp.nf, (int32_t)rp.nf});
+                rstats.push_back(StatsJob{rp.rs, (int32_t)rp.nf, 0, rp.ds, (int32_t)rp.nf, 0, (int32_t)rp.nf,
+                                          (int32_t)rp.nf, nullptr, nullptr, rp.st, rp.st + NB, rp.st + 2 * NB,
+                                          rp.st + 3 * NB});
+                s.trace.n_cells += NB * rp.nf;
+            }
+        }
+        // ---- 7: realigned spectrograms and statistics ------------------------
+        if (!copies.empty()) launch_copy_frames(upload(copies), (int)copies.size(), nbi, max_cols, stream_);
+        run_gammatone(rjobs);
+        if (!rprep.empty()) launch_prep(upload(rprep), (int)rprep.size(), nbi, stream_);
+        if (!rstats.empty()) launch_stats(upload(rstats), (int)rstats.size(), nbi, stream_);
+        std::vector<double *> h_rst;
+        for (auto &s : ps) {
+            if (!s.live) continue;
+            for (auto &rp : s.rps) {
+                if (rp.nf == 0) continue;
+                double *h = pinned_.alloc_n<double>(3 * NB + 1);
+                d2h(h, rp.st, (3 * NB + 1) * sizeof(double));
+                h_rst.push_back(h);
+            }
+        }
+        record(events_[6]);
+        sync();
+
+        // ---- 8: accept rule (reference src/realign.zig:398-460) --------------
+        size_t q = 0;
+        for (auto &s : ps) {
+            if (!s.live) continue;
+            for (auto &rp : s.rps) {
+                if (rp.nf == 0) continue;
+                const double *st = h_rst[q++];
+                host::Match &m = s.matches[rp.mi];
+                const double sim = st[3 * NB];
+                if (!(sim < m.similarity)) {
+                    m.means.assign(st, st + NB);
+                    m.stddevs.assign(st + NB, st + 2 * NB);
+                    m.energy.assign(st + 2 * NB, st + 3 * NB);
+                    m.similarity = sim;
+                    const double dur = (double)rp.trim.len / (double)sample_rate;
+                    if (rp.trim.lag_seconds > 0.0)
+                        m.ref_start += rp.trim.lag_seconds;
+                    else
+                        m.deg_start -= rp.trim.lag_seconds;
+                    m.ref_end = m.ref_start + dur;
+                    m.deg_end = m.deg_start + dur;
+                    s.trace.realign_accepted[rp.mi] = 1;
+                }
+            }
+        }
+    }
+    record(events_[7]);
+    VQB_CUDA(cudaEventSynchronize(events_[7]));
+    for (uint64_t g = 0; g < timing_.gammatone_launches; ++g)
+        timing_.gammatone_kernel_ms += elapsed(gt_events_[2 * g], gt_events_[2 * g + 1]);
+    timing_.kernel_launches = launch_counter() - launches0;
+
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        PairOutcome &o = out[i];
+        if (!s.live) {
+            o.code = s.code;
+            o.message = s.msg;
+            continue;
+        }
+        try {
+            s.trace.n_rms_window = W;
+            o.scores = host::build_scores(std::move(s.matches), NB, fd, svr_.get(), opt_.speech, opt_.unscaled_speech,
+                                          rc.fb.cf, s.al.lag_seconds);
+            o.trace = std::move(s.trace);
+        } catch (const Error &e) {
+            o.code = e.code;
+            o.message = e.what();
+        }
+    }
+    timing_.total_ms = elapsed(events_[0], events_[7]);
+    timing_.lag_ms = elapsed(events_[0], events_[1]);
+    timing_.spectrogram_ms = elapsed(events_[2], events_[3]);
+    timing_.prep_ms = elapsed(events_[3], events_[4]);
+    timing_.nsim_ms = elapsed(events_[4], events_[5]);
+    timing_.realign_ms = n_slices ? elapsed(events_[5], events_[6]) : 0.0;
+}
+
+}  // namespace vqb

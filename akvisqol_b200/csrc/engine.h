@@ -1,0 +1,156 @@
+// Batched ViSQOL pipeline on one GPU.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "host_model.h"
+
+namespace vqb {
+
+struct Options {
+    bool speech = false;
+    int32_t radius = 60;
+    bool unscaled_speech = false;
+    bool disable_global_alignment = false;
+    bool disable_realignment = false;
+};
+
+struct PairTrace {
+    int64_t global_lag = 0;
+    double spl_factor = 1.0;
+    uint64_t deg_len = 0, nf_ref = 0, nf_deg = 0;
+    std::vector<int64_t> ref_index, deg_offset, realign_lag, realign_frames;
+    std::vector<uint8_t> valid, realign_reused, realign_accepted;
+    uint64_t n_rms = 0, n_rms_window = 0, n_cells = 0;
+    double fft_nlogn = 0;
+};
+
+struct PairOutcome {
+    int code = 0;
+    std::string message;
+    host::Scores scores;
+    PairTrace trace;
+};
+
+struct Timing {
+    double total_ms = 0, lag_ms = 0, spectrogram_ms = 0, prep_ms = 0, nsim_ms = 0, realign_ms = 0;
+    double gammatone_kernel_ms = 0;
+    uint64_t gammatone_launches = 0, gammatone_rms = 0, gammatone_window = 0;
+    uint64_t kernel_launches = 0, h2d_bytes = 0, d2h_bytes = 0, host_syncs = 0;
+};
+
+// Device memory that grows by whole chunks and is recycled per batch.
+class Arena {
+public:
+    ~Arena();
+    void reset();
+    void *alloc(size_t bytes);
+    template <class T>
+    T *alloc_n(size_t n) {
+        return static_cast<T *>(alloc(n * sizeof(T)));
+    }
+    size_t reserved() const;
+
+private:
+    struct Chunk {
+        char *base;
+        size_t size, used;
+    };
+    std::vector<Chunk> chunks_;
+    size_t current_ = 0;
+};
+
+// Page-locked host memory with the same policy.
+class PinnedArena {
+public:
+    ~PinnedArena();
+    void reset();
+    void *alloc(size_t bytes);
+    template <class T>
+    T *alloc_n(size_t n) {
+        return static_cast<T *>(alloc(n * sizeof(T)));
+    }
+
+private:
+    struct Chunk {
+        char *base;
+        size_t size, used;
+    };
+    std::vector<Chunk> chunks_;
+    size_t current_ = 0;
+};
+
+class Engine {
+public:
+    Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr);
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    // Score n pairs at one sample rate. Pointers are host memory unless
+    // device_inputs. Per-pair failures land in out[i].code.
+    void measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
+                       const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
+                       std::vector<PairOutcome> &out);
+
+    const Timing &last_timing() const { return timing_; }
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Single-stage entry points (device buffers, exact form).
+    void spectrogram(const host::Filterbank &fb, const double *d_hann, size_t window, size_t hop, const double *d_x,
+                     size_t len, double *d_out, size_t nf);
+    void lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags);
+    const double2 *twiddles(size_t n);
+
+private:
+    struct RateCache {
+        host::Filterbank fb;
+        host::Geometry geo;
+        BandCoeffs *d_coeffs = nullptr;
+        double *d_hann = nullptr;
+    };
+    const RateCache &rate_cache(uint32_t sample_rate);
+
+    // Envelope (or raw) lag search for jobs whose a/b/stat pointers are set;
+    // lags land in the jobs' lag_out (device). Launches only.
+    void launch_lag_jobs(std::vector<LagJob> &jobs, bool raw);
+    template <class T>
+    T *upload(const std::vector<T> &v);
+    void *upload_bytes(const void *src, size_t bytes);
+    void d2h(void *dst, const void *src, size_t bytes);
+    void sync();
+    void record(cudaEvent_t e);
+    float elapsed(cudaEvent_t a, cudaEvent_t b);
+
+    int device_;
+    Options opt_;
+    std::shared_ptr<const host::Svr> svr_;
+    size_t nb_, patch_;
+    double max_freq_;
+    cudaStream_t stream_ = nullptr;
+    Arena arena_;
+    PinnedArena pinned_;
+    std::map<uint32_t, RateCache> rates_;
+    std::map<size_t, double2 *> twiddles_;
+    std::vector<cudaEvent_t> events_;
+    cudaEvent_t gt_events_[4] = {};  // begin/end of up to two gammatone launches
+    Timing timing_;
+};
+
+// CUDA call check: throws Error(kBackend) with the call and message.
+void cuda_check(cudaError_t e, const char *what);
+
+// The calling thread's visqol_last_error() text.
+void set_last_error(const std::string &message);
+#define VQB_CUDA(call) ::vqb::cuda_check((call), #call)
+
+}  // namespace vqb

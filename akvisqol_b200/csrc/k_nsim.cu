@@ -1,0 +1,241 @@
+// NSIM patch similarity (reference src/nsim.zig) for the DP table and the
+// per-match band statistics.
+//
+// Table: NSIM of every reference patch at every degraded offset in its
+// search window (reference src/accel.zig:126-146, measureSimilarityAt
+// src/nsim.zig:364-424). One thread owns one (patch, offset) and walks the
+// patch's cells in row-major order, so its serial sum is the CPU's order.
+// The threads of a CTA share one reference patch: its values and its
+// precomputed terms (3x3 mean, mean², variance) sit in shared memory and
+// are read as broadcasts; the degraded plane's terms come from global
+// memory, and neighbouring threads read neighbouring offsets (coalesced).
+// Interior patch columns reuse the plane's terms, whose 3x3 neighbourhood
+// is the patch's; the two edge columns are recomputed with the patch's
+// replicate padding, as the CPU does.
+#include "device.cuh"
+#include "kernels.h"
+
+namespace vqb {
+
+namespace {
+
+// Degraded plane of one pair: the prepared spectrogram zero-padded to
+// `width` frames, its 3x3 mean, mean² and variance (reference
+// src/nsim.zig:236-263). out arrays are nb x width.
+__global__ void __launch_bounds__(256) plane_kernel(const PlaneJob *__restrict__ jobs, int nb) {
+    const PlaneJob job = jobs[blockIdx.y];
+    const int w = job.width, nf = job.nf;
+    const int total = nb * w;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int r = e / w, c = e - r * w;
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        const int cm = c == 0 ? 0 : c - 1, cp = c + 1 >= w ? w - 1 : c + 1;
+        auto P = [&](int rr, int cc) -> double { return cc < nf ? job.spec[(int64_t)rr * nf + cc] : 0.0; };
+        const double p00 = P(rm, cm), p01 = P(rm, c), p02 = P(rm, cp);
+        const double p10 = P(r, cm), p11 = P(r, c), p12 = P(r, cp);
+        const double p20 = P(rp, cm), p21 = P(rp, c), p22 = P(rp, cp);
+        const double mu = taps9(p00, p01, p02, p10, p11, p12, p20, p21, p22);
+        const double csq = taps9(p00 * p00, p01 * p01, p02 * p02, p10 * p10, p11 * p11, p12 * p12, p20 * p20,
+                                 p21 * p21, p22 * p22);
+        const double dms = mu * mu;
+        job.pad[e] = p11;
+        job.mu[e] = mu;
+        job.dms[e] = dms;
+        job.sds[e] = csq - dms;
+    }
+}
+
+// Reference-patch terms (reference precomputeRef, src/nsim.zig:318-329):
+// out[4][nb][P] = {patch values, 3x3 mean, mean², conv(x²) - mean²}.
+__global__ void __launch_bounds__(256) ref_terms_kernel(const RefTermsJob *__restrict__ jobs, int nb, int P) {
+    const RefTermsJob job = jobs[blockIdx.y];
+    const int total = nb * P;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int r = e / P, c = e - r * P;
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        const int cm = c == 0 ? 0 : c - 1, cp = c + 1 >= P ? P - 1 : c + 1;
+        auto R = [&](int rr, int cc) -> double { return job.spec[(int64_t)rr * job.nf + job.col + cc]; };
+        const double p00 = R(rm, cm), p01 = R(rm, c), p02 = R(rm, cp);
+        const double p10 = R(r, cm), p11 = R(r, c), p12 = R(r, cp);
+        const double p20 = R(rp, cm), p21 = R(rp, c), p22 = R(rp, cp);
+        const double mu = taps9(p00, p01, p02, p10, p11, p12, p20, p21, p22);
+        const double csq = taps9(p00 * p00, p01 * p01, p02 * p02, p10 * p10, p11 * p11, p12 * p12, p20 * p20,
+                                 p21 * p21, p22 * p22);
+        const double rms = mu * mu;
+        job.out[e] = p11;
+        job.out[total + e] = mu;
+        job.out[2 * total + e] = rms;
+        job.out[3 * total + e] = csq - rms;
+    }
+}
+
+constexpr int kTableThreads = 128;
+
+// One thread per (patch, offset); CTA = one patch x 128 offsets.
+__global__ void __launch_bounds__(kTableThreads) table_kernel(const TableTask *__restrict__ tasks, int nb, int P) {
+    extern __shared__ double sm[];
+    const TableTask t = tasks[blockIdx.x];
+    const int total = nb * P;
+    for (int e = threadIdx.x; e < 4 * total; e += blockDim.x) sm[e] = t.ref_terms[e];
+    __syncthreads();
+    const int64_t off = t.off0 + threadIdx.x;
+    if (off > t.hi) return;
+    const double *rv = sm, *mr = sm + total, *rms = sm + 2 * total, *srs = sm + 3 * total;
+    const int w = t.width;
+    const double *pad = t.pad, *mu = t.mu, *dmsp = t.dms, *sdsp = t.sds;
+    double sum = 0.0;
+    for (int r = 0; r < nb; ++r) {
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        const double *pm = pad + (int64_t)rm * w + off, *p0 = pad + (int64_t)r * w + off,
+                     *pp = pad + (int64_t)rp * w + off;
+        const double *qm = rv + rm * P, *q0 = rv + r * P, *qp = rv + rp * P;
+        // ref x deg products of the 3 rows, columns (c-1, c, c+1) clamped
+        // to the patch; slid along c.
+        double am = qm[0] * pm[0], a0 = q0[0] * p0[0], ap = qp[0] * pp[0];  // column cm
+        double bm = am, b0 = a0, bp = ap;                                   // column c
+        for (int c = 0; c < P; ++c) {
+            const int cp = c + 1 >= P ? P - 1 : c + 1;
+            const double cm_ = qm[cp] * pm[cp], c0 = q0[cp] * p0[cp], cpp = qp[cp] * pp[cp];
+            // Taps.row over the patch's ref x deg products.
+            const double crd = taps9(am, bm, cm_, a0, b0, c0, ap, bp, cpp);
+            double md, dms, sds;
+            if (c == 0 || c == P - 1) {
+                const int cmi = c == 0 ? 0 : c - 1;
+                const double d00 = pm[cmi], d01 = pm[c], d02 = pm[cp];
+                const double d10 = p0[cmi], d11 = p0[c], d12 = p0[cp];
+                const double d20 = pp[cmi], d21 = pp[c], d22 = pp[cp];
+                md = taps9(d00, d01, d02, d10, d11, d12, d20, d21, d22);
+                const double cdsq = taps9(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12,
+                                          d20 * d20, d21 * d21, d22 * d22);
+                dms = md * md;
+                sds = cdsq - dms;
+            } else {
+                const int64_t pi = (int64_t)r * w + off + c;
+                md = mu[pi];
+                dms = dmsp[pi];
+                sds = sdsp[pi];
+            }
+            const int ri = r * P + c;
+            sum += sim_cell(mr[ri], rms[ri], srs[ri], md, dms, sds, crd);
+            // slide: column c becomes cm, column cp becomes c
+            am = bm, a0 = b0, ap = bp;
+            bm = cm_, b0 = c0, bp = cpp;
+        }
+    }
+    t.out[off] = sum / (double)(nb * P);
+}
+
+// Per-band statistics of one patch pair, one thread per band row
+// (reference measurePatchSimilarity, src/nsim.zig:427-510). Cell values are
+// formed from the 3x3 neighbourhood on the fly and recomputed for the
+// stddev pass (same operations, same bits).
+__global__ void __launch_bounds__(32) stats_kernel(const StatsJob *__restrict__ jobs, int nb) {
+    const StatsJob job = jobs[blockIdx.x];
+    const int r = threadIdx.x;
+    __shared__ double means_sm[32];
+    int deg_col = job.deg_col;
+    bool valid = true, reached = true;
+    if (job.dp_offset) {
+        const int64_t o = *job.dp_offset;
+        reached = o >= 0;
+        valid = *job.dp_valid != 0;
+        deg_col = (int)(o < 0 ? 0 : o);
+    }
+    const int nc = job.ncols;
+    if (!reached) {
+        // Patches the backtrack never reached keep zeroed statistics.
+        if (r < nb) job.means[r] = job.stddevs[r] = job.energy[r] = 0.0;
+        if (r == 0) *job.similarity = 0.0;
+        return;
+    }
+    auto R = [&](int rr, int cc) -> double { return job.ref[(int64_t)rr * job.ref_stride + job.ref_col + cc]; };
+    auto D = [&](int rr, int cc) -> double {
+        return deg_col + cc < job.deg_cols ? job.deg[(int64_t)rr * job.deg_stride + deg_col + cc] : 0.0;
+    };
+    double mean = 0.0;
+    if (r < nb) {
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        const double inv_ncols = 1.0 / (double)nc;
+        auto cell = [&](int c) -> double {
+            const int cm = c == 0 ? 0 : c - 1, cp = c + 1 >= nc ? nc - 1 : c + 1;
+            const double r00 = R(rm, cm), r01 = R(rm, c), r02 = R(rm, cp), r10 = R(r, cm), r11 = R(r, c),
+                         r12 = R(r, cp), r20 = R(rp, cm), r21 = R(rp, c), r22 = R(rp, cp);
+            const double d00 = D(rm, cm), d01 = D(rm, c), d02 = D(rm, cp), d10 = D(r, cm), d11 = D(r, c),
+                         d12 = D(r, cp), d20 = D(rp, cm), d21 = D(rp, c), d22 = D(rp, cp);
+            const double mr = taps9(r00, r01, r02, r10, r11, r12, r20, r21, r22);
+            const double md = taps9(d00, d01, d02, d10, d11, d12, d20, d21, d22);
+            const double crs = taps9(r00 * r00, r01 * r01, r02 * r02, r10 * r10, r11 * r11, r12 * r12, r20 * r20,
+                                     r21 * r21, r22 * r22);
+            const double cds = taps9(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12, d20 * d20,
+                                     d21 * d21, d22 * d22);
+            const double crd = taps9(r00 * d00, r01 * d01, r02 * d02, r10 * d10, r11 * d11, r12 * d12, r20 * d20,
+                                     r21 * d21, r22 * d22);
+            const double rms = mr * mr, dms = md * md;
+            return sim_cell(mr, rms, crs - rms, md, dms, cds - dms, crd);
+        };
+        double deg_sum = 0.0;
+        for (int c = 0; c < nc; ++c) deg_sum += D(r, c);
+        job.energy[r] = deg_sum * inv_ncols;
+        double sim_sum = 0.0;
+        for (int c = 0; c < nc; ++c) sim_sum += cell(c);
+        mean = sim_sum * inv_ncols;
+        double sd = 0.0;
+        if (nc > 1) {
+            double ss = 0.0;
+            for (int c = 0; c < nc; ++c) {
+                const double diff = cell(c) - mean;
+                ss += diff * diff;
+            }
+            sd = sqrt(ss / ((double)nc - 1.0));
+        }
+        job.stddevs[r] = sd;
+        job.means[r] = valid ? mean : 0.0;
+        means_sm[r] = mean;
+    }
+    __syncthreads();
+    if (r == 0) {
+        double acc = 0.0;
+        for (int b = 0; b < nb; ++b) acc += means_sm[b];
+        *job.similarity = valid ? acc / (double)nb : 0.0;
+    }
+}
+
+}  // namespace
+
+void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int total = nb * max_width;
+    int blocks = (total + 255) / 256;
+    if (blocks > 1024) blocks = 1024;
+    plane_kernel<<<dim3((unsigned)blocks, (unsigned)njobs), 256, 0, s>>>(d_jobs, nb);
+    launch_counter() += 1;
+}
+
+void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int total = nb * P;
+    const int blocks = (total + 255) / 256;
+    ref_terms_kernel<<<dim3((unsigned)blocks, (unsigned)njobs), 256, 0, s>>>(d_jobs, nb, P);
+    launch_counter() += 1;
+}
+
+int table_offsets_per_cta() { return kTableThreads; }
+
+void nsim_init_attributes() {
+    cudaFuncSetAttribute(table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, cudaStream_t s) {
+    if (ntasks <= 0) return;
+    const size_t smem = (size_t)4 * nb * P * sizeof(double);
+    table_kernel<<<ntasks, kTableThreads, smem, s>>>(d_tasks, nb, P);
+    launch_counter() += 1;
+}
+
+void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s) {
+    if (njobs <= 0) return;
+    stats_kernel<<<njobs, 32, 0, s>>>(d_jobs, nb);
+    launch_counter() += 1;
+}
+
+}  // namespace vqb

@@ -1,0 +1,264 @@
+// Signal-level kernels: serial reductions in the CPU's order, upper
+// envelopes packed for the lag FFT, and the lag/SPL application.
+//
+// The reference sums signals left to right in f64 (envelope mean and
+// Nyquist term, src/envelope.zig:28-41; SPL energy, src/audio.zig:132-136).
+// A parallel tree would round differently, so each reduction runs as one
+// warp per signal: the warp loads 32 consecutive samples (one coalesced
+// 256-byte read), forms the per-sample terms in parallel, and every lane
+// then adds the 32 terms in index order from register shuffles. The add
+// chain is the only serial part; many signals run side by side.
+#include "device.cuh"
+#include "kernels.h"
+
+namespace vqb {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+enum SumKind : int {
+    kSumAndEnergy = 0,  // out[0] = sum x, out[2] = sum x*x
+    kNyquist = 1,       // out[1] = sum (-1)^k (x - out[0]/len); reads out[0]
+    kEnergy = 2,        // out[2] = sum x*x
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(128) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= njobs) return;
+    const SumJob job = jobs[warp];
+    const int64_t len = job.sig.len;
+    const double mean = KIND == kNyquist ? job.out[0] / (double)len : 0.0;
+    double acc0 = 0.0, acc1 = 0.0;
+    // Software pipeline: the next chunk's load is in flight while the
+    // current chunk's terms are added.
+    double next = lane < len ? vsig_at(job.sig, lane) : 0.0;
+    for (int64_t base = 0; base < len; base += 32) {
+        const double v = next;
+        const int64_t k = base + lane;
+        if (base + 32 < len) next = (k + 32 < len) ? vsig_at(job.sig, k + 32) : 0.0;
+        double t0, t1 = 0.0;
+        if (KIND == kSumAndEnergy) {
+            t0 = v;
+            t1 = v * v;
+        } else if (KIND == kNyquist) {
+            const double d = v - mean;
+            t0 = (k & 1) ? -d : d;
+        } else {
+            t0 = v * v;
+        }
+        const int64_t left = len - base;
+        if (left >= 32) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                acc0 += __shfl_sync(kFull, t0, j);
+                if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
+            }
+        } else {
+            for (int j = 0; j < (int)left; ++j) {
+                acc0 += __shfl_sync(kFull, t0, j);
+                if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
+            }
+        }
+    }
+    if (lane == 0) {
+        if (KIND == kSumAndEnergy) {
+            job.out[0] = acc0;
+            job.out[2] = acc1;
+        } else if (KIND == kNyquist) {
+            job.out[1] = acc0;
+        } else {
+            job.out[2] = acc0;
+        }
+    }
+}
+
+// Energy of the lag-aligned degraded signal (reference src/realign.zig:91-110
+// then src/audio.zig:132-136): applyLag drops -lag leading samples, or
+// prepends lag zeros (which add +0 to the sum), and leaves lags of 0 or
+// beyond half the reference alone. The lag is read on the device.
+struct AlignedEnergyArgs {
+    VSig deg;
+    int64_t ref_len;
+    const int64_t *lag;
+    double *out;  // [energy, aligned length]
+};
+
+__global__ void __launch_bounds__(128) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs, int njobs) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= njobs) return;
+    const AlignedEnergyArgs job = jobs[warp];
+    const int64_t lag = *job.lag;
+    const int64_t half_ref = job.ref_len / 2;
+    const int64_t mag = lag < 0 ? -lag : lag;
+    const int64_t L = job.deg.len;
+    int64_t skip = 0, alen = L;
+    if (lag != 0 && mag <= half_ref) {
+        if (lag < 0) {
+            skip = -lag < L ? -lag : L;
+            alen = L - skip;
+        } else {
+            alen = L + lag;
+        }
+    }
+    double acc = 0.0;
+    const int64_t n = L - skip;
+    double next = lane < n ? vsig_at(job.deg, skip + lane) : 0.0;
+    for (int64_t base = 0; base < n; base += 32) {
+        const double v = next;
+        const int64_t k = base + lane;
+        if (base + 32 < n) next = (k + 32 < n) ? vsig_at(job.deg, skip + k + 32) : 0.0;
+        const double t = v * v;
+        const int64_t left = n - base;
+        if (left >= 32) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) acc += __shfl_sync(kFull, t, j);
+        } else {
+            for (int j = 0; j < (int)left; ++j) acc += __shfl_sync(kFull, t, j);
+        }
+    }
+    if (lane == 0) {
+        job.out[0] = acc;
+        job.out[1] = (double)alen;
+    }
+}
+
+__host__ __device__ inline int64_t next_pow_two(int64_t x) {
+    int64_t n = 1;
+    while (n < x) n <<= 1;
+    return n;
+}
+
+// upperEnvelope's closed form (reference src/envelope.zig:23-53) for both
+// signals of a lag job, packed as z = env_a + i env_b zero-padded to n
+// (reference src/xcorr.zig:204-208). raw: the signals themselves.
+template <bool RAW>
+__global__ void __launch_bounds__(256) pack_kernel(const LagJob *__restrict__ jobs, int njobs) {
+    const LagJob job = jobs[blockIdx.y];
+    const int64_t n = job.n;
+    double mean_a = 0, q_a = 0, mean_b = 0, q_b = 0;
+    if (!RAW) {
+        const int64_t la = job.a.len, lb = job.b.len;
+        if (la > 0) {
+            mean_a = job.stats_a[0] / (double)la;
+            const int64_t Na = next_pow_two(la) > 32 ? next_pow_two(la) : 32;
+            q_a = job.stats_a[1] / (double)Na;
+        }
+        if (lb > 0) {
+            mean_b = job.stats_b[0] / (double)lb;
+            const int64_t Nb = next_pow_two(lb) > 32 ? next_pow_two(lb) : 32;
+            q_b = job.stats_b[1] / (double)Nb;
+        }
+    }
+    const double eps = 0.000001;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        if (i < job.a.len) {
+            const double x = vsig_at(job.a, i);
+            if (RAW) {
+                re = x;
+            } else {
+                const double pc = x - mean_a;
+                const double nt = (i & 1) ? -q_a : q_a;
+                re = fabs(2.0 * (pc - nt) - eps) + mean_a;
+            }
+        }
+        if (i < job.b.len) {
+            const double x = vsig_at(job.b, i);
+            if (RAW) {
+                im = x;
+            } else {
+                const double pc = x - mean_b;
+                const double nt = (i & 1) ? -q_b : q_b;
+                im = fabs(2.0 * (pc - nt) - eps) + mean_b;
+            }
+        }
+        job.z[i] = make_double2(re, im);
+    }
+}
+
+// out[i] = aligned(i) * factor: scaleToMatchSpl on the lag-aligned signal
+// (reference src/audio.zig:152-158; x * 1.0 == x when unscaled).
+struct ScaleArgs {
+    VSig src;
+    double factor;
+    double *out;
+};
+
+__global__ void __launch_bounds__(256) scale_kernel(const ScaleArgs *__restrict__ jobs, int njobs) {
+    const ScaleArgs job = jobs[blockIdx.y];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < job.src.len;
+         i += (int64_t)gridDim.x * blockDim.x)
+        job.out[i] = vsig_at(job.src, i) * job.factor;
+}
+
+}  // namespace
+
+uint64_t &launch_counter() {
+    static thread_local uint64_t count = 0;
+    return count;
+}
+
+void launch_envelope_stats(const SumJob *d_jobs, int njobs, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int per_block = 4;
+    const int grid = (njobs + per_block - 1) / per_block;
+    serial_sum_kernel<kSumAndEnergy><<<grid, 32 * per_block, 0, s>>>(d_jobs, njobs);
+    serial_sum_kernel<kNyquist><<<grid, 32 * per_block, 0, s>>>(d_jobs, njobs);
+    launch_counter() += 2;
+}
+
+void launch_energy(const SumJob *d_jobs, int njobs, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int per_block = 4;
+    serial_sum_kernel<kEnergy><<<(njobs + per_block - 1) / per_block, 32 * per_block, 0, s>>>(d_jobs, njobs);
+    launch_counter() += 1;
+}
+
+void launch_aligned_energy(const void *d_args, int njobs, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int per_block = 4;
+    aligned_energy_kernel<<<(njobs + per_block - 1) / per_block, 32 * per_block, 0, s>>>(
+        static_cast<const AlignedEnergyArgs *>(d_args), njobs);
+    launch_counter() += 1;
+}
+
+size_t aligned_energy_args_size() { return sizeof(AlignedEnergyArgs); }
+
+void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out) {
+    AlignedEnergyArgs a{deg, ref_len, d_lag, d_out};
+    *static_cast<AlignedEnergyArgs *>(dst) = a;
+}
+
+void launch_pack(const LagJob *d_jobs, int njobs, int64_t max_n, bool raw, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int threads = 256;
+    int64_t blocks = (max_n + threads - 1) / threads;
+    if (blocks > 4096) blocks = 4096;
+    dim3 grid((unsigned)blocks, (unsigned)njobs);
+    if (raw)
+        pack_kernel<true><<<grid, threads, 0, s>>>(d_jobs, njobs);
+    else
+        pack_kernel<false><<<grid, threads, 0, s>>>(d_jobs, njobs);
+    launch_counter() += 1;
+}
+
+size_t scale_args_size() { return sizeof(ScaleArgs); }
+void fill_scale_args(void *dst, const VSig &src, double factor, double *out) {
+    *static_cast<ScaleArgs *>(dst) = ScaleArgs{src, factor, out};
+}
+void launch_scale(const void *d_args, int njobs, int64_t max_len, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int threads = 256;
+    int64_t blocks = (max_len + threads - 1) / threads;
+    if (blocks > 2048) blocks = 2048;
+    if (blocks < 1) blocks = 1;
+    scale_kernel<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(static_cast<const ScaleArgs *>(d_args),
+                                                                            njobs);
+    launch_counter() += 1;
+}
+
+}  // namespace vqb

@@ -1,0 +1,93 @@
+// Kernel launchers and the job records they read (device memory).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace vqb {
+
+// Degraded plane of one pair (reference src/nsim.zig:224-263).
+struct PlaneJob {
+    const double *spec;  // prepared degraded spectrogram, nb x nf
+    int32_t nf, width;
+    double *pad, *mu, *dms, *sds;  // nb x width each
+};
+
+// Reference-patch terms: spec columns [col, col+P) of a prepared
+// spectrogram with nf frames; out is 4 x nb x P.
+struct RefTermsJob {
+    const double *spec;
+    int32_t nf, col;
+    double *out;
+};
+
+// NSIM table block: offsets [off0, min(off0+127, hi)] of one patch.
+struct TableTask {
+    const double *ref_terms;  // 4 x nb x P
+    const double *pad, *mu, *dms, *sds;
+    int32_t width;
+    int32_t off0, hi;
+    double *out;  // row of the table: out[off]
+};
+
+// DP of one pair over its sims table (np x nf_deg).
+struct DpJob {
+    const double *sims;
+    const int64_t *lo, *hi;
+    int32_t np;
+    int64_t nf_deg;
+    double *dp;
+    int64_t *bt;
+    int64_t *offset;  // np: matched offset, -1 when not reached
+    uint8_t *valid;   // np
+};
+
+// Kernels launched by this thread so far (each launcher counts its own).
+uint64_t &launch_counter();
+
+// k_signal.cu
+void launch_envelope_stats(const SumJob *d_jobs, int njobs, cudaStream_t s);
+void launch_energy(const SumJob *d_jobs, int njobs, cudaStream_t s);
+size_t aligned_energy_args_size();
+void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out);
+void launch_aligned_energy(const void *d_args, int njobs, cudaStream_t s);
+void launch_pack(const LagJob *d_jobs, int njobs, int64_t max_n, bool raw, cudaStream_t s);
+size_t scale_args_size();
+void fill_scale_args(void *dst, const VSig &src, double factor, double *out);
+void launch_scale(const void *d_args, int njobs, int64_t max_len, cudaStream_t s);
+
+// k_fft.cu
+void fft_init_attributes();
+void launch_fft(double2 *z, int64_t n, bool inverse, const double2 *top, int njobs, int64_t stride, cudaStream_t s);
+void launch_cross(double2 *z, int64_t n, int njobs, int64_t stride, cudaStream_t s);
+int argmax_parts(int64_t n);
+void launch_argmax(const double2 *z, const LagJob *d_jobs, int njobs, int64_t n, int64_t stride, double *pv,
+                   int64_t *pk, cudaStream_t s);
+
+// k_gammatone.cu
+int gammatone_frames_per_cta(int nb);
+size_t gammatone_tile_size();
+void fill_gammatone_tile(void *dst, int job, int frame0);
+void launch_gammatone(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const BandCoeffs *d_coeffs, int nb,
+                      const double *d_hann, int window, int hop, cudaStream_t s);
+void launch_copy_frames(const CopyJob *d_jobs, int njobs, int nb, int max_cols, cudaStream_t s);
+
+// k_spec.cu
+void launch_prep(const PrepJob *d_jobs, int njobs, int nb, cudaStream_t s);
+void launch_log10(const double *x, int64_t n, double *out, cudaStream_t s);
+
+// k_nsim.cu
+void nsim_init_attributes();
+void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cudaStream_t s);
+void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaStream_t s);
+int table_offsets_per_cta();
+void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, cudaStream_t s);
+void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s);
+
+// k_dp.cu
+void launch_dp(const DpJob *d_jobs, int njobs, cudaStream_t s);
+
+}  // namespace vqb

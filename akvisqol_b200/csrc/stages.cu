@@ -1,0 +1,224 @@
+// Single-stage entry points of include/visqol_b200.h: each copies host
+// buffers in, runs one kernel family of the batch pipeline, and copies the
+// result out. They exist so that each kernel can be checked on its own
+// against the CPU model; the batch pipeline does not use them.
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/visqol_b200.h"
+#include "engine.h"
+#include "host_model.h"
+#include "kernels.h"
+
+using vqb::Error;
+
+namespace {
+
+int stage_fail(int code, const char *m) {
+    vqb::set_last_error(m);
+    return code;
+}
+
+// Device buffer freed on scope exit.
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    explicit DBuf(size_t n) { VQB_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T))); }
+    DBuf(const T *h, size_t n) : DBuf(n) {
+        if (n) VQB_CUDA(cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    ~DBuf() { cudaFree(p); }
+    void get(T *h, size_t n) const {
+        if (n) VQB_CUDA(cudaMemcpy(h, p, n * sizeof(T), cudaMemcpyDeviceToHost));
+    }
+};
+
+// One engine per process for the stage calls (its stream and caches).
+vqb::Engine &stage_engine() {
+    static std::mutex mu;
+    static std::unique_ptr<vqb::Engine> e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!e) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        e = std::make_unique<vqb::Engine>(dev, vqb::Options{}, nullptr);
+    }
+    return *e;
+}
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        f();
+        VQB_CUDA(cudaGetLastError());
+        VQB_CUDA(cudaDeviceSynchronize());
+        return VISQOL_OK;
+    } catch (const Error &e) {
+        stage_fail(e.code, e.what());
+        return e.code;
+    } catch (const std::exception &e) {
+        stage_fail(VISQOL_E_INTERNAL, e.what());
+        return VISQOL_E_INTERNAL;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int visqol_b200_spectrogram(size_t nb, const double *coeffs, const double *hann, size_t window, size_t hop,
+                            const double *x, size_t len, double *out, size_t *nf_out) {
+    if (!coeffs || !hann || (!x && len) || !out || !nf_out || nb == 0 || nb > 32 || hop == 0)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        vqb::host::Filterbank fb;
+        fb.nb = nb;
+        fb.coeffs.assign(coeffs, coeffs + 8 * nb);
+        for (size_t b = 0; b < nb; ++b) fb.run.push_back(vqb::host::band_coeffs(coeffs + 8 * b));
+        const size_t nf = vqb::host::num_frames(len, window, hop);
+        *nf_out = nf;
+        DBuf<double> dx(x, len), dh(hann, window), dout(nb * nf);
+        stage_engine().spectrogram(fb, dh.p, window, hop, dx.p, len, dout.p, nf);
+        dout.get(out, nb * nf);
+    });
+}
+
+static int lag_stage(const double *a, size_t la, const double *b, size_t lb, int64_t *lag, bool raw) {
+    if ((!a && la) || (!b && lb) || !lag) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        DBuf<double> da(a, la), db(b, lb);
+        const vqb::VSig va{da.p, 0, (int64_t)la, (int64_t)la}, vb{db.p, 0, (int64_t)lb, (int64_t)lb};
+        stage_engine().lags(1, &va, &vb, raw, lag);
+    });
+}
+
+int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t lb, int64_t *lag) {
+    return lag_stage(a, la, b, lb, lag, false);
+}
+
+int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb, int64_t *lag) {
+    return lag_stage(a, la, b, lb, lag, true);
+}
+
+int visqol_b200_fft(double *buf, size_t n, int inverse) {
+    if (!buf || n == 0 || (n & (n - 1))) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "n must be a power of two");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double2> z(reinterpret_cast<const double2 *>(buf), n);
+        vqb::launch_fft(z.p, (int64_t)n, inverse != 0, e.twiddles(n), 1, (int64_t)n, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        z.get(reinterpret_cast<double2 *>(buf), n);
+    });
+}
+
+int visqol_b200_prepare_for_comparison(double *ref, double *deg, size_t nb, size_t nfr, size_t nfd) {
+    if ((!ref && nfr) || (!deg && nfd) || nb == 0) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double> ri(ref, nb * nfr), di(deg, nb * nfd), ro(nb * nfr), dout(nb * nfd);
+        vqb::PrepJob pj{ri.p, di.p, ro.p, dout.p, (int32_t)nfr, (int32_t)nfd};
+        DBuf<vqb::PrepJob> dj(&pj, 1);
+        vqb::launch_prep(dj.p, 1, (int)nb, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        ro.get(ref, nb * nfr);
+        dout.get(deg, nb * nfd);
+    });
+}
+
+int visqol_b200_log10(const double *x, size_t n, double *out) {
+    if ((!x || !out) && n) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double> dx(x, n), dy(n);
+        vqb::launch_log10(dx.p, (int64_t)n, dy.p, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        dy.get(out, n);
+    });
+}
+
+int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref, const double *deg_spec, size_t nf_deg, size_t nb,
+                           size_t patch, size_t np, const int64_t *ref_idx, const int64_t *lo, const int64_t *hi,
+                           double *out) {
+    if (!ref_spec || !deg_spec || !ref_idx || !lo || !hi || !out || nb == 0 || patch == 0)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    for (size_t p = 0; p < np; ++p)
+        if (lo[p] < 0 || hi[p] < lo[p] || (size_t)hi[p] >= nf_deg || ref_idx[p] < 0 ||
+            (size_t)ref_idx[p] + patch > nf_ref)
+            return stage_fail(VISQOL_E_INVALID_ARGUMENT, "patch window out of range");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        size_t width = nf_deg;
+        for (size_t p = 0; p < np; ++p) width = std::max(width, (size_t)hi[p] + patch);
+        DBuf<double> rs(ref_spec, nb * nf_ref), ds(deg_spec, nb * nf_deg), plane(4 * nb * width),
+            terms(np * 4 * nb * patch), sims(np * nf_deg);
+        VQB_CUDA(cudaMemset(sims.p, 0, std::max<size_t>(1, np * nf_deg) * sizeof(double)));
+        const size_t pl = nb * width;
+        vqb::PlaneJob pj{ds.p, (int32_t)nf_deg, (int32_t)width, plane.p, plane.p + pl, plane.p + 2 * pl, plane.p + 3 * pl};
+        std::vector<vqb::RefTermsJob> tj;
+        std::vector<vqb::TableTask> tasks;
+        for (size_t p = 0; p < np; ++p) {
+            double *t = terms.p + p * 4 * nb * patch;
+            tj.push_back(vqb::RefTermsJob{rs.p, (int32_t)nf_ref, (int32_t)ref_idx[p], t});
+            for (int64_t o = lo[p]; o <= hi[p]; o += vqb::table_offsets_per_cta())
+                tasks.push_back(vqb::TableTask{t, pj.pad, pj.mu, pj.dms, pj.sds, (int32_t)width, (int32_t)o,
+                                               (int32_t)hi[p], sims.p + p * nf_deg});
+        }
+        DBuf<vqb::PlaneJob> dpj(&pj, 1);
+        DBuf<vqb::RefTermsJob> dtj(tj.data(), tj.size());
+        DBuf<vqb::TableTask> dtasks(tasks.data(), tasks.size());
+        vqb::launch_plane(dpj.p, 1, (int)nb, (int)width, e.stream());
+        vqb::launch_ref_terms(dtj.p, (int)tj.size(), (int)nb, (int)patch, e.stream());
+        vqb::launch_table(dtasks.p, (int)tasks.size(), (int)nb, (int)patch, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        sims.get(out, np * nf_deg);
+    });
+}
+
+int visqol_b200_dp(const double *sims, size_t np, size_t nf_deg, const int64_t *lo, const int64_t *hi,
+                   int64_t *offset, uint8_t *valid, size_t *reached) {
+    if (!sims || !lo || !hi || !offset || !valid || np == 0) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    for (size_t p = 0; p < np; ++p)
+        if (lo[p] < 0 || hi[p] < lo[p] || (size_t)hi[p] >= nf_deg || (p && lo[p] < lo[p - 1]))
+            return stage_fail(VISQOL_E_INVALID_ARGUMENT, "window out of range");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double> ds(sims, np * nf_deg), dpb(np * nf_deg);
+        DBuf<int64_t> dlo(lo, np), dhi(hi, np), bt(np * nf_deg), off(np);
+        DBuf<uint8_t> val(np);
+        vqb::DpJob job{ds.p, dlo.p, dhi.p, (int32_t)np, (int64_t)nf_deg, dpb.p, bt.p, off.p, val.p};
+        DBuf<vqb::DpJob> dj(&job, 1);
+        vqb::launch_dp(dj.p, 1, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        off.get(offset, np);
+        val.get(valid, np);
+        size_t r = 0;
+        for (size_t p = 0; p < np; ++p) r += offset[p] >= 0;
+        if (reached) *reached = r;
+    });
+}
+
+int visqol_b200_patch_similarity(const double *ref, const double *deg, size_t nrows, size_t ncols, double *means,
+                                 double *stddevs, double *deg_energy, double *mean) {
+    if (!ref || !deg || !means || !stddevs || !deg_energy || !mean || nrows == 0 || nrows > 32 || ncols == 0)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double> dr(ref, nrows * ncols), dd(deg, nrows * ncols), st(3 * nrows + 1);
+        vqb::StatsJob job{dr.p, (int32_t)ncols, 0, dd.p, (int32_t)ncols, 0, (int32_t)ncols, (int32_t)ncols,
+                          nullptr, nullptr, st.p, st.p + nrows, st.p + 2 * nrows, st.p + 3 * nrows};
+        DBuf<vqb::StatsJob> dj(&job, 1);
+        vqb::launch_stats(dj.p, 1, (int)nrows, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        std::vector<double> h(3 * nrows + 1);
+        st.get(h.data(), h.size());
+        std::memcpy(means, h.data(), nrows * sizeof(double));
+        std::memcpy(stddevs, h.data() + nrows, nrows * sizeof(double));
+        std::memcpy(deg_energy, h.data() + 2 * nrows, nrows * sizeof(double));
+        *mean = h[3 * nrows];
+    });
+}
+
+}  // extern "C"

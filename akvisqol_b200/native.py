@@ -1,0 +1,453 @@
+"""ctypes binding of libvisqol (include/visqol.h + include/visqol_b200.h).
+
+Mirrors the reference's Python binding (src/python/visqol/_native.py:32-248):
+the same ``Options``/``Patch``/``Result`` structures, ``Context`` with
+``measure``/``measure_batch``/``measure_files``/``measure_files_batch``,
+``NativeError`` carrying the C error code, and ``free``/``vec`` helpers, so
+code written against that module reads the same here. Extensions: traced
+batches (per-pair lags and matches), device-resident inputs, per-stage
+timing, and single-stage calls.
+
+There is no fallback: if ``libvisqol.so`` is missing, importing this module
+raises ImportError.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import (POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_size_t, c_uint8, c_uint32,
+                    c_uint64, c_void_p)
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libvisqol.so"
+
+MODE_AUDIO = 0
+MODE_SPEECH = 1
+BACKENDS = {"cpu": 0, "metal": 1, "cuda": 2, "vulkan": 3}
+PRECISIONS = {"exact": 0, "fast": 1, "balanced": 2, "auto": 3}
+
+OK = 0
+E_INVALID_ARGUMENT = -1
+E_OUT_OF_MEMORY = -2
+E_IO = -3
+E_MODEL = -4
+E_SIGNAL = -5
+E_BACKEND = -6
+E_INTERNAL = -7
+
+DEVICE_INPUTS = 1
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("mode", c_uint32), ("search_window_radius", c_int32),
+        ("use_unscaled_speech_mos_mapping", c_uint8), ("disable_global_alignment", c_uint8),
+        ("disable_realignment", c_uint8), ("use_lattice_model", c_uint8),
+        ("model_path", c_char_p), ("backend", c_uint32), ("precision", c_uint32),
+    ]
+
+
+class Patch(ctypes.Structure):
+    _fields_ = [
+        ("similarity", c_double), ("ref_patch_start_time", c_double), ("ref_patch_end_time", c_double),
+        ("deg_patch_start_time", c_double), ("deg_patch_end_time", c_double),
+        ("freq_band_means", POINTER(c_double)), ("freq_band_stddevs", POINTER(c_double)),
+        ("freq_band_deg_energy", POINTER(c_double)),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("moslqo", c_double), ("vnsim", c_double), ("alignment_lag_s", c_double), ("num_bands", c_size_t),
+        ("fvnsim", POINTER(c_double)), ("fvnsim10", POINTER(c_double)), ("fstdnsim", POINTER(c_double)),
+        ("fvdegenergy", POINTER(c_double)), ("center_freq_bands", POINTER(c_double)),
+        ("num_patches", c_size_t), ("patch_sims", POINTER(Patch)),
+    ]
+
+
+class Trace(ctypes.Structure):
+    _fields_ = [
+        ("global_lag", c_int64), ("spl_factor", c_double), ("deg_len", c_uint64),
+        ("nf_ref", c_uint64), ("nf_deg", c_uint64), ("num_patches", c_uint64),
+        ("ref_index", POINTER(c_int64)), ("deg_offset", POINTER(c_int64)), ("valid", POINTER(c_uint8)),
+        ("realign_lag", POINTER(c_int64)), ("realign_frames", POINTER(c_int64)),
+        ("realign_reused", POINTER(c_uint8)), ("realign_accepted", POINTER(c_uint8)),
+        ("n_rms", c_uint64), ("n_rms_window", c_uint64), ("n_cells", c_uint64), ("fft_nlogn", c_double),
+    ]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [
+        ("total_ms", c_double), ("lag_ms", c_double), ("spectrogram_ms", c_double), ("prep_ms", c_double),
+        ("nsim_ms", c_double), ("realign_ms", c_double), ("gammatone_kernel_ms", c_double),
+        ("gammatone_launches", c_uint64), ("gammatone_rms", c_uint64), ("gammatone_window", c_uint64),
+        ("kernel_launches", c_uint64), ("h2d_bytes", c_uint64), ("d2h_bytes", c_uint64), ("host_syncs", c_uint64),
+    ]
+
+
+def build() -> Path:
+    """Compile libvisqol.so with the package Makefile (no-op when current)."""
+    subprocess.run(["make", "-s", "-j8", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def _load() -> ctypes.CDLL:
+    override = os.environ.get("VISQOL_B200_LIBRARY")
+    path = Path(override) if override else LIB_PATH
+    if not path.is_file():
+        raise ImportError(f"libvisqol not found at {path}; build it with `make -C {HERE}`")
+    lib = ctypes.CDLL(str(path))
+    D, I64, SZ, U8 = POINTER(c_double), POINTER(c_int64), POINTER(c_size_t), POINTER(c_uint8)
+    sig = {
+        "visqol_abi_version": (c_uint32, []),
+        "visqol_version": (c_char_p, []),
+        "visqol_last_error": (c_char_p, []),
+        "visqol_available_backends": (c_uint32, []),
+        "visqol_options_default": (None, [POINTER(Options)]),
+        "visqol_create": (c_int, [POINTER(Options), POINTER(c_void_p)]),
+        "visqol_destroy": (None, [c_void_p]),
+        "visqol_measure": (c_int, [c_void_p, D, c_size_t, D, c_size_t, c_uint32, POINTER(POINTER(Result))]),
+        "visqol_measure_files": (c_int, [c_void_p, c_char_p, c_char_p, POINTER(POINTER(Result))]),
+        "visqol_measure_batch": (c_int, [c_void_p, c_size_t, POINTER(D), SZ, POINTER(D), SZ, c_uint32, c_uint32,
+                                         POINTER(POINTER(Result)), POINTER(c_int32)]),
+        "visqol_measure_files_batch": (c_int, [c_void_p, c_size_t, POINTER(c_char_p), POINTER(c_char_p), c_uint32,
+                                               POINTER(POINTER(Result)), POINTER(c_int32)]),
+        "visqol_result_free": (None, [POINTER(Result)]),
+        "visqol_b200_measure_batch": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, POINTER(c_void_p), SZ,
+                                              c_uint32, c_uint32, POINTER(POINTER(Result)), POINTER(c_int32),
+                                              POINTER(POINTER(Trace))]),
+        "visqol_b200_trace_free": (None, [POINTER(Trace)]),
+        "visqol_b200_last_timing": (c_int, [c_void_p, POINTER(Timing)]),
+        "visqol_b200_device_info": (c_int, [c_int, c_char_p, c_size_t, POINTER(c_int), POINTER(c_int),
+                                            POINTER(c_int)]),
+        "visqol_b200_spectrogram": (c_int, [c_size_t, D, D, c_size_t, c_size_t, D, c_size_t, D, SZ]),
+        "visqol_b200_envelope_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
+        "visqol_b200_best_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
+        "visqol_b200_fft": (c_int, [D, c_size_t, c_int]),
+        "visqol_b200_prepare_for_comparison": (c_int, [D, D, c_size_t, c_size_t, c_size_t]),
+        "visqol_b200_log10": (c_int, [D, c_size_t, D]),
+        "visqol_b200_nsim_table": (c_int, [D, c_size_t, D, c_size_t, c_size_t, c_size_t, c_size_t, I64, I64, I64, D]),
+        "visqol_b200_dp": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
+        "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
+        "visqol_b200_peak": (c_int, [c_int, D]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+ABI_VERSION = 1
+if lib.visqol_abi_version() != ABI_VERSION:
+    raise ImportError(f"libvisqol ABI {lib.visqol_abi_version()} does not match the bindings ({ABI_VERSION})")
+
+__version__ = lib.visqol_version().decode()
+
+# Every symbol include/visqol.h and include/visqol_b200.h declare.
+EXPORTS = [
+    "visqol_abi_version", "visqol_version", "visqol_last_error", "visqol_available_backends",
+    "visqol_options_default", "visqol_create", "visqol_destroy", "visqol_measure", "visqol_measure_files",
+    "visqol_measure_batch", "visqol_measure_files_batch", "visqol_result_free",
+    "visqol_b200_measure_batch", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
+    "visqol_b200_spectrogram", "visqol_b200_envelope_lag", "visqol_b200_best_lag", "visqol_b200_fft",
+    "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
+    "visqol_b200_patch_similarity", "visqol_b200_peak",
+]
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+def last_error(code: int) -> NativeError:
+    return NativeError(code, (lib.visqol_last_error() or b"").decode(errors="replace"))
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise last_error(rc)
+
+
+def available_backends() -> list[str]:
+    mask = lib.visqol_available_backends()
+    return [name for name, bit in BACKENDS.items() if mask & (1 << bit)]
+
+
+def as_signal(x, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    if a.ndim != 1:
+        raise ValueError(f"{name} must be a 1-D mono signal, got shape {a.shape}")
+    return a
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def _i64(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_int64))
+
+
+class Context:
+    """Owns a ``visqol_ctx`` (one thread at a time)."""
+
+    def __init__(self, *, mode: int = MODE_AUDIO, search_window_radius: int = 60,
+                 use_unscaled_speech_mos_mapping: bool = False, disable_global_alignment: bool = False,
+                 disable_realignment: bool = False, use_lattice_model: bool = False, model_path: str | None = None,
+                 backend: str = "cuda", precision: str | None = None):
+        if backend not in BACKENDS:
+            raise ValueError(f"unknown backend {backend!r}; expected one of {sorted(BACKENDS)}")
+        if precision is not None and precision not in PRECISIONS:
+            raise ValueError(f"unknown precision {precision!r}; expected one of {sorted(PRECISIONS)}")
+        opts = Options()
+        lib.visqol_options_default(ctypes.byref(opts))
+        opts.mode = mode
+        opts.search_window_radius = search_window_radius
+        opts.use_unscaled_speech_mos_mapping = int(bool(use_unscaled_speech_mos_mapping))
+        opts.disable_global_alignment = int(bool(disable_global_alignment))
+        opts.disable_realignment = int(bool(disable_realignment))
+        opts.use_lattice_model = int(bool(use_lattice_model))
+        opts.model_path = os.fsencode(model_path) if model_path else None
+        opts.backend = BACKENDS[backend]
+        if precision is not None:
+            opts.precision = PRECISIONS[precision]
+        handle = c_void_p()
+        _check(lib.visqol_create(ctypes.byref(opts), ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            lib.visqol_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def measure(self, ref: np.ndarray, deg: np.ndarray, sample_rate: int):
+        out = POINTER(Result)()
+        _check(lib.visqol_measure(self._handle, _ptr(ref), ref.size, _ptr(deg), deg.size, sample_rate,
+                                  ctypes.byref(out)))
+        return out
+
+    def measure_files(self, ref_path: str, deg_path: str):
+        out = POINTER(Result)()
+        _check(lib.visqol_measure_files(self._handle, os.fsencode(ref_path), os.fsencode(deg_path),
+                                        ctypes.byref(out)))
+        return out
+
+    def measure_batch(self, refs: list[np.ndarray], degs: list[np.ndarray], sample_rate: int, num_threads: int = 0):
+        n = len(refs)
+        ref_ptrs = (POINTER(c_double) * n)(*[_ptr(a) for a in refs])
+        deg_ptrs = (POINTER(c_double) * n)(*[_ptr(a) for a in degs])
+        ref_lens = (c_size_t * n)(*[a.size for a in refs])
+        deg_lens = (c_size_t * n)(*[a.size for a in degs])
+        outs = (POINTER(Result) * n)()
+        status = (c_int32 * n)()
+        lib.visqol_measure_batch(self._handle, n, ref_ptrs, ref_lens, deg_ptrs, deg_lens, sample_rate, num_threads,
+                                 outs, status)
+        return _collect(outs, status, n)
+
+    def measure_files_batch(self, ref_paths: list[str], deg_paths: list[str], num_threads: int = 0):
+        n = len(ref_paths)
+        refs = (c_char_p * n)(*[os.fsencode(p) for p in ref_paths])
+        degs = (c_char_p * n)(*[os.fsencode(p) for p in deg_paths])
+        outs = (POINTER(Result) * n)()
+        status = (c_int32 * n)()
+        lib.visqol_measure_files_batch(self._handle, n, refs, degs, num_threads, outs, status)
+        return _collect(outs, status, n)
+
+    def measure_batch_traced(self, refs, degs, sample_rate: int, device_inputs: bool = False,
+                             ref_lens=None, deg_lens=None):
+        """Batch with per-pair traces. Host arrays, or device addresses (ints)
+        with their lengths when ``device_inputs``. Returns a list of
+        ``(code, result dict or None, trace dict or None)``."""
+        n = len(refs)
+        if device_inputs:
+            rp = (c_void_p * n)(*[int(a) for a in refs])
+            dp = (c_void_p * n)(*[int(a) for a in degs])
+            rl = (c_size_t * n)(*ref_lens)
+            dl = (c_size_t * n)(*deg_lens)
+        else:
+            rp = (c_void_p * n)(*[a.ctypes.data for a in refs])
+            dp = (c_void_p * n)(*[a.ctypes.data for a in degs])
+            rl = (c_size_t * n)(*[a.size for a in refs])
+            dl = (c_size_t * n)(*[a.size for a in degs])
+        outs = (POINTER(Result) * n)()
+        traces = (POINTER(Trace) * n)()
+        status = (c_int32 * n)()
+        lib.visqol_b200_measure_batch(self._handle, n, rp, rl, dp, dl, sample_rate,
+                                      DEVICE_INPUTS if device_inputs else 0, outs, status, traces)
+        res = []
+        for i in range(n):
+            if status[i] == OK:
+                res.append((OK, result_dict(outs[i].contents), trace_dict(traces[i].contents)))
+                free(outs[i])
+                lib.visqol_b200_trace_free(traces[i])
+            else:
+                res.append((status[i], None, None))
+        return res
+
+    def last_timing(self) -> dict:
+        t = Timing()
+        _check(lib.visqol_b200_last_timing(self._handle, ctypes.byref(t)))
+        return {name: getattr(t, name) for name, _ in Timing._fields_}
+
+
+def _collect(outs, status, n: int) -> list:
+    """Per-pair ``Result`` pointers, or ``NativeError`` for failed pairs."""
+    return [outs[i] if status[i] == OK else NativeError(status[i], f"pair {i}: error code {status[i]}")
+            for i in range(n)]
+
+
+def free(result) -> None:
+    lib.visqol_result_free(result)
+
+
+def vec(ptr, n: int) -> np.ndarray:
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0)
+
+
+def result_dict(r: Result) -> dict:
+    nb, npch = r.num_bands, r.num_patches
+    patches = []
+    for i in range(npch):
+        p = r.patch_sims[i]
+        patches.append({
+            "similarity": p.similarity, "ref_patch_start_time": p.ref_patch_start_time,
+            "ref_patch_end_time": p.ref_patch_end_time, "deg_patch_start_time": p.deg_patch_start_time,
+            "deg_patch_end_time": p.deg_patch_end_time, "freq_band_means": vec(p.freq_band_means, nb),
+            "freq_band_stddevs": vec(p.freq_band_stddevs, nb), "freq_band_deg_energy": vec(p.freq_band_deg_energy, nb),
+        })
+    return {
+        "moslqo": r.moslqo, "vnsim": r.vnsim, "alignment_lag_s": r.alignment_lag_s, "num_bands": nb,
+        "fvnsim": vec(r.fvnsim, nb), "fvnsim10": vec(r.fvnsim10, nb), "fstdnsim": vec(r.fstdnsim, nb),
+        "fvdegenergy": vec(r.fvdegenergy, nb), "center_freq_bands": vec(r.center_freq_bands, nb),
+        "patch_sims": patches,
+    }
+
+
+def _arr(ptr, n, dtype):
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, dtype)
+
+
+def trace_dict(t: Trace) -> dict:
+    n = t.num_patches
+    return {
+        "global_lag": t.global_lag, "spl_factor": t.spl_factor, "deg_len": t.deg_len,
+        "nf_ref": t.nf_ref, "nf_deg": t.nf_deg, "num_patches": n,
+        "ref_index": _arr(t.ref_index, n, np.int64), "deg_offset": _arr(t.deg_offset, n, np.int64),
+        "valid": _arr(t.valid, n, np.uint8), "realign_lag": _arr(t.realign_lag, n, np.int64),
+        "realign_frames": _arr(t.realign_frames, n, np.int64), "realign_reused": _arr(t.realign_reused, n, np.uint8),
+        "realign_accepted": _arr(t.realign_accepted, n, np.uint8),
+        "n_rms": t.n_rms, "n_rms_window": t.n_rms_window, "n_cells": t.n_cells, "fft_nlogn": t.fft_nlogn,
+    }
+
+
+def device_info(device: int = 0) -> dict:
+    name = ctypes.create_string_buffer(256)
+    sm, ma, mi = c_int(), c_int(), c_int()
+    _check(lib.visqol_b200_device_info(device, name, 256, ctypes.byref(sm), ctypes.byref(ma), ctypes.byref(mi)))
+    return {"name": name.value.decode(), "sm_count": sm.value, "cc": (ma.value, mi.value)}
+
+
+def peak_tflops(kind: int) -> float:
+    """Measured pipe peak: 0 f64 mul/add (no FMA), 1 f64 FMA, 2 f32 FMA."""
+    t = c_double()
+    _check(lib.visqol_b200_peak(kind, ctypes.byref(t)))
+    return t.value
+
+
+# ---- single-stage calls (exact f64 kernels on host buffers) ----------------
+
+def spectrogram(x, coeffs: np.ndarray, hann: np.ndarray, window: int, hop: int) -> np.ndarray:
+    x = as_signal(x, "x")
+    c = np.ascontiguousarray(coeffs, dtype=np.float64).reshape(-1)
+    h = np.ascontiguousarray(hann, dtype=np.float64)
+    nb = c.size // 8
+    nf_max = 0 if x.size < window else 1 + (x.size - window) // hop
+    out = np.zeros(max(1, nb * nf_max))
+    nf = c_size_t()
+    _check(lib.visqol_b200_spectrogram(nb, _ptr(c), _ptr(h), window, hop, _ptr(x), x.size, _ptr(out),
+                                       ctypes.byref(nf)))
+    return out[: nb * nf.value].reshape(nb, nf.value)
+
+
+def envelope_lag(a, b) -> int:
+    a, b = as_signal(a, "a"), as_signal(b, "b")
+    lag = c_int64()
+    _check(lib.visqol_b200_envelope_lag(_ptr(a), a.size, _ptr(b), b.size, ctypes.byref(lag)))
+    return lag.value
+
+
+def best_lag(a, b) -> int:
+    a, b = as_signal(a, "a"), as_signal(b, "b")
+    lag = c_int64()
+    _check(lib.visqol_b200_best_lag(_ptr(a), a.size, _ptr(b), b.size, ctypes.byref(lag)))
+    return lag.value
+
+
+def fft(z: np.ndarray, inverse: bool = False) -> np.ndarray:
+    buf = np.ascontiguousarray(z, dtype=np.complex128).copy()
+    _check(lib.visqol_b200_fft(buf.ctypes.data_as(POINTER(c_double)), buf.size, int(inverse)))
+    return buf
+
+
+def prepare_for_comparison(ref: np.ndarray, deg: np.ndarray):
+    r = np.ascontiguousarray(ref, dtype=np.float64).copy()
+    d = np.ascontiguousarray(deg, dtype=np.float64).copy()
+    _check(lib.visqol_b200_prepare_for_comparison(_ptr(r), _ptr(d), r.shape[0], r.shape[1], d.shape[1]))
+    return r, d
+
+
+def log10x10(x) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros_like(x)
+    _check(lib.visqol_b200_log10(_ptr(x), x.size, _ptr(out)))
+    return out
+
+
+def nsim_table(ref_spec, deg_spec, patch: int, ref_idx, lo, hi) -> np.ndarray:
+    rs = np.ascontiguousarray(ref_spec, dtype=np.float64)
+    ds = np.ascontiguousarray(deg_spec, dtype=np.float64)
+    nb, nfr = rs.shape
+    nfd = ds.shape[1]
+    ri = np.ascontiguousarray(ref_idx, dtype=np.int64)
+    lo = np.ascontiguousarray(lo, dtype=np.int64)
+    hi = np.ascontiguousarray(hi, dtype=np.int64)
+    out = np.zeros(max(1, ri.size * nfd))
+    _check(lib.visqol_b200_nsim_table(_ptr(rs), nfr, _ptr(ds), nfd, nb, patch, ri.size, _i64(ri), _i64(lo),
+                                      _i64(hi), _ptr(out)))
+    return out[: ri.size * nfd].reshape(ri.size, nfd)
+
+
+def dp(sims, lo, hi):
+    s = np.ascontiguousarray(sims, dtype=np.float64)
+    np_, nfd = s.shape
+    lo = np.ascontiguousarray(lo, dtype=np.int64)
+    hi = np.ascontiguousarray(hi, dtype=np.int64)
+    off = np.zeros(np_, np.int64)
+    valid = np.zeros(np_, np.uint8)
+    reached = c_size_t()
+    _check(lib.visqol_b200_dp(_ptr(s), np_, nfd, _i64(lo), _i64(hi), _i64(off),
+                              valid.ctypes.data_as(POINTER(c_uint8)), ctypes.byref(reached)))
+    return off, valid, reached.value
+
+
+def patch_similarity(ref, deg):
+    r = np.ascontiguousarray(ref, dtype=np.float64)
+    d = np.ascontiguousarray(deg, dtype=np.float64)
+    nr, nc = r.shape
+    means, sd, en, mean = np.zeros(nr), np.zeros(nr), np.zeros(nr), c_double()
+    _check(lib.visqol_b200_patch_similarity(_ptr(r), _ptr(d), nr, nc, _ptr(means), _ptr(sd), _ptr(en),
+                                            ctypes.byref(mean)))
+    return mean.value, means, sd, en

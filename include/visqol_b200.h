@@ -1,0 +1,142 @@
+/* akvisqol_b200 extensions to the ViSQOL C ABI (include/visqol.h).
+ *
+ * Entry points the reference has no C declaration for but that a host
+ * binding this backend needs: batches with device-resident inputs and the
+ * discrete decisions of each pair (the reference's backend.Engine
+ * measureBatch, src/backend.zig:78-82, and its GPU pipeline's lag/match
+ * read-backs, src/gpu/pipeline.zig:223-283), per-stage device timing, and
+ * single-stage entry points that run one kernel family on host buffers (the
+ * reference's accel.Cpu stage jobs, src/accel.zig:21-146). Plain pointers
+ * and sizes only. All functions return VISQOL_OK or a negative visqol.h
+ * error code and set visqol_last_error().
+ */
+#ifndef VISQOL_B200_H
+#define VISQOL_B200_H
+
+#include "visqol.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* visqol_b200_measure_batch flags. */
+enum {
+    /* refs/degs are device pointers (cudaMalloc'd on the context's GPU). */
+    VISQOL_B200_DEVICE_INPUTS = 1u << 0,
+};
+
+/* Discrete decisions and work counts of one measured pair. */
+typedef struct {
+    int64_t global_lag;            /* envelope xcorr lag in samples (0 if not run) */
+    double spl_factor;             /* degraded SPL scale factor, 1 when unscaled */
+    uint64_t deg_len;              /* aligned degraded length */
+    uint64_t nf_ref, nf_deg;       /* spectrogram frames */
+    uint64_t num_patches;
+    const int64_t *ref_index;      /* per patch: reference start frame */
+    const int64_t *deg_offset;     /* per patch: DP-matched degraded frame */
+    const uint8_t *valid;          /* per patch: DP match valid */
+    const int64_t *realign_lag;    /* per patch: slice envelope lag (0 if not run) */
+    const int64_t *realign_frames; /* per patch: trimmed frames, -1 if not run */
+    const uint8_t *realign_reused; /* per patch: bit0 ref / bit1 deg frames copied */
+    const uint8_t *realign_accepted;
+    uint64_t n_rms;                /* gammatone (frame, band) evaluations */
+    uint64_t n_rms_window;         /* samples per evaluation */
+    uint64_t n_cells;              /* NSIM cells evaluated */
+    double fft_nlogn;              /* sum of n*log2(n) over complex FFTs */
+} visqol_b200_trace;
+
+/* Device time of the last batch on a context, by stage (CUDA events on the
+ * context's stream), plus the counts behind the roofline figures. */
+typedef struct {
+    double total_ms;               /* first launch to last result copy */
+    double lag_ms;                 /* envelopes, FFT xcorr, argmax (global) */
+    double spectrogram_ms;         /* gammatone of full signals */
+    double prep_ms;                /* dB, floors, joint minimum */
+    double nsim_ms;                /* planes, NSIM table, DP, match stats */
+    double realign_ms;             /* slice lags, realigned spectrograms, stats */
+    double gammatone_kernel_ms;    /* sum of gammatone kernel durations */
+    uint64_t gammatone_launches;
+    uint64_t gammatone_rms;        /* (frame, band) RMS evaluations launched */
+    uint64_t gammatone_window;     /* samples per evaluation */
+    uint64_t kernel_launches;      /* all kernels of the batch */
+    uint64_t h2d_bytes, d2h_bytes;
+    uint64_t host_syncs;
+} visqol_b200_timing;
+
+/* Score n pairs as visqol_measure_batch does; with traces non-NULL,
+ * traces[i] receives pair i's decisions (free with visqol_b200_trace_free).
+ * flags: VISQOL_B200_DEVICE_INPUTS. */
+int visqol_b200_measure_batch(visqol_ctx *ctx, size_t n,
+                              const double *const *refs, const size_t *ref_lens,
+                              const double *const *degs, const size_t *deg_lens,
+                              uint32_t sample_rate, uint32_t flags,
+                              visqol_result **out, int32_t *status,
+                              visqol_b200_trace **traces);
+void visqol_b200_trace_free(visqol_b200_trace *trace);
+int visqol_b200_last_timing(visqol_ctx *ctx, visqol_b200_timing *out);
+
+/* Device name, SM count and compute capability of the context's GPU. */
+int visqol_b200_device_info(int device, char *name, size_t name_len,
+                            int *sm_count, int *cc_major, int *cc_minor);
+
+/* Measured arithmetic peak of the current GPU in TFLOP/s, the denominator
+ * of the roofline fractions: kind 0 = f64 multiply and add as separate
+ * instructions (the exact form's arithmetic), 1 = f64 FMA, 2 = f32 FMA. */
+int visqol_b200_peak(int kind, double *tflops);
+
+/* ---- single-stage entry points (host buffers in and out, exact f64) ----
+ * Each runs the same kernels the batch pipeline uses. */
+
+/* Gammatone spectrogram, row-major [nb][nf] (reference
+ * src/gammatone.zig:432-467). coeffs: nb x {a0,a11,a12,a13,a14,b1,b2,gain}
+ * ascending. Returns the frame count in *nf. */
+int visqol_b200_spectrogram(size_t nb, const double *coeffs, const double *hann,
+                            size_t window, size_t hop, const double *x, size_t len,
+                            double *out, size_t *nf);
+
+/* Upper-envelope FFT cross-correlation lag (reference src/accel.zig:100-107,
+ * src/xcorr.zig:197-251). */
+int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t lb,
+                             int64_t *lag);
+
+/* Raw-signal FFT cross-correlation lag (reference src/xcorr.zig:197-251). */
+int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb,
+                         int64_t *lag);
+
+/* Unscaled radix-2 DIF forward (natural in, bit-reversed out) and DIT
+ * inverse, in place on n interleaved complex values (reference
+ * src/dsp/fft.zig:127-166). */
+int visqol_b200_fft(double *buf, size_t n, int inverse);
+
+/* dB, per-frame floor, joint minimum in place (reference
+ * src/spectrogram.zig:69-80). */
+int visqol_b200_prepare_for_comparison(double *ref, double *deg, size_t nb,
+                                       size_t nf_ref, size_t nf_deg);
+
+/* 10*log10 as the dB conversion computes it on the device. */
+int visqol_b200_log10(const double *x, size_t n, double *out);
+
+/* NSIM of each reference patch at each degraded offset in [lo, hi]:
+ * out[p*nf_deg + off] (reference src/accel.zig:126-146). */
+int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref,
+                           const double *deg_spec, size_t nf_deg, size_t nb,
+                           size_t patch, size_t np, const int64_t *ref_idx,
+                           const int64_t *lo, const int64_t *hi, double *out);
+
+/* DP and backtrack over a similarity table (reference src/dp.zig:216-352):
+ * matched offset and validity per patch; *reached counts patches visited. */
+int visqol_b200_dp(const double *sims, size_t np, size_t nf_deg,
+                   const int64_t *lo, const int64_t *hi,
+                   int64_t *offset, uint8_t *valid, size_t *reached);
+
+/* Per-band NSIM statistics of one patch pair (reference
+ * src/nsim.zig:427-510); *mean gets the mean of the band means. */
+int visqol_b200_patch_similarity(const double *ref, const double *deg,
+                                 size_t nrows, size_t ncols, double *means,
+                                 double *stddevs, double *deg_energy, double *mean);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VISQOL_B200_H */

@@ -1,0 +1,175 @@
+"""End-to-end parity of the GPU pipeline (exact form) with the oracle,
+through the C ABI: |dMOS| <= 1e-12, and every discrete decision identical
+(global lag, frames, patch indices, DP offsets, per-patch realignment lags,
+frame reuse, accept decisions)."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MOS_TOL = 1e-12
+FEATURE_TOL = 1e-12
+
+
+def assert_same(res, tr, want, wtr, tol=FEATURE_TOL):
+    assert abs(res["moslqo"] - want["moslqo"]) <= MOS_TOL
+    assert abs(res["vnsim"] - want["vnsim"]) <= tol
+    assert res["alignment_lag_s"] == want["alignment_lag_s"]
+    for key in ("fvnsim", "fvnsim10", "fstdnsim", "fvdegenergy"):
+        assert np.max(np.abs(res[key] - want[key])) <= tol, key
+    assert np.array_equal(res["center_freq_bands"], want["center_freq_bands"])
+    assert tr["global_lag"] == wtr["global_lag"]
+    assert tr["spl_factor"] == wtr["spl_factor"]
+    for key in ("deg_len", "nf_ref", "nf_deg", "num_patches"):
+        assert tr[key] == wtr[key], key
+    for key in ("ref_index", "deg_offset", "valid", "realign_lag", "realign_frames", "realign_reused",
+                "realign_accepted"):
+        assert np.array_equal(tr[key], wtr[key]), key
+    assert tr["n_rms"] == wtr["n_rms"] and tr["n_cells"] == wtr["n_cells"]
+    assert len(res["patch_sims"]) == len(want["patch_sims"])
+    for g, w in zip(res["patch_sims"], want["patch_sims"]):
+        for key in ("ref_patch_start_time", "ref_patch_end_time", "deg_patch_start_time", "deg_patch_end_time"):
+            assert g[key] == w[key], key
+        assert abs(g["similarity"] - w["similarity"]) <= tol
+        for key in ("freq_band_means", "freq_band_stddevs", "freq_band_deg_energy"):
+            assert np.max(np.abs(g[key] - w[key])) <= tol, key
+
+
+@pytest.fixture(scope="module")
+def audio_ctx(native):
+    return native.Context(mode=native.MODE_AUDIO, precision="exact")
+
+
+@pytest.fixture(scope="module")
+def speech_ctx(native):
+    return native.Context(mode=native.MODE_SPEECH, use_lattice_model=False, precision="exact")
+
+
+def run(ctx, pairs, sr):
+    return ctx.measure_batch_traced([p[0] for p in pairs], [p[1] for p in pairs], sr)
+
+
+def test_audio_10s_48k_pair(native, oracle, audio_ctx):
+    from akvisqol_b200 import synth
+    ref, deg = synth.audio_pair(synth.SEED_BASE)
+    (code, res, tr), = run(audio_ctx, [(ref, deg)], 48000)
+    assert code == 0
+    want, wtr = oracle.measure(ref, deg, 48000)
+    assert_same(res, tr, want, wtr)
+
+
+def test_speech_8s_16k_pair(native, oracle, speech_ctx):
+    from akvisqol_b200 import synth
+    ref, deg = synth.speech_pair(synth.SEED_BASE)
+    (code, res, tr), = run(speech_ctx, [(ref, deg)], 16000)
+    assert code == 0
+    want, wtr = oracle.measure(ref, deg, 16000, oracle.options(mode=1))
+    assert_same(res, tr, want, wtr)
+
+
+def test_uneven_audio_batch(native, oracle, audio_ctx):
+    from akvisqol_b200 import synth
+    pairs = synth.audio_batch(6, min_s=2.0, max_s=9.0)
+    got = run(audio_ctx, pairs, 48000)
+    for (ref, deg), (code, res, tr) in zip(pairs, got):
+        want, wtr = oracle.measure(ref, deg, 48000)
+        assert code == 0
+        assert_same(res, tr, want, wtr)
+
+
+def test_speech_batch(native, oracle, speech_ctx):
+    from akvisqol_b200 import synth
+    pairs = synth.speech_batch(4, min_s=2.0, max_s=6.0)
+    got = run(speech_ctx, pairs, 16000)
+    for (ref, deg), (code, res, tr) in zip(pairs, got):
+        try:
+            want, wtr = oracle.measure(ref, deg, 16000, oracle.options(mode=1))
+        except oracle.OracleError as e:
+            assert code == e.code
+            continue
+        assert code == 0
+        assert_same(res, tr, want, wtr)
+
+
+def test_batch_equals_single(native, audio_ctx):
+    from akvisqol_b200 import synth
+    pairs = [synth.audio_pair(synth.SEED_BASE + i, seconds=3.0) for i in range(3)]
+    batch = run(audio_ctx, pairs, 48000)
+    for (ref, deg), (code, res, tr) in zip(pairs, batch):
+        single = native.result_dict(audio_ctx.measure(native.as_signal(ref, "r"), native.as_signal(deg, "d"), 48000).contents)
+        assert res["moslqo"] == single["moslqo"]
+        assert np.array_equal(res["fvnsim"], single["fvnsim"])
+
+
+def test_identical_signals(native, oracle, audio_ctx):
+    from akvisqol_b200 import synth
+    ref, _ = synth.audio_pair(synth.SEED_BASE + 7, seconds=4.0)
+    (code, res, tr), = run(audio_ctx, [(ref, ref.copy())], 48000)
+    want, wtr = oracle.measure(ref, ref, 48000)
+    assert code == 0 and tr["global_lag"] == 0
+    assert_same(res, tr, want, wtr)
+
+
+def test_sine_plus_noise(native, oracle, audio_ctx):
+    # the reference Python suite's sine smoke case (src/python/tests/test_visqol_lib_py.py:50-62)
+    ref = np.sin(np.linspace(0.0, 1000, 48000 * 2))
+    deg = ref + np.random.default_rng(0).normal(size=ref.shape)
+    (code, res, tr), = run(audio_ctx, [(ref, deg)], 48000)
+    want, wtr = oracle.measure(ref, deg, 48000)
+    assert code == 0 and 1.0 <= res["moslqo"] < 5.0
+    assert_same(res, tr, want, wtr)
+
+
+def test_per_pair_errors(native, audio_ctx):
+    from akvisqol_b200 import synth
+    good = synth.audio_pair(synth.SEED_BASE + 3, seconds=2.5)
+    pairs = [good, (np.zeros(100), np.zeros(100)), (np.zeros(0), np.zeros(0)), good]
+    got = run(audio_ctx, pairs, 48000)
+    assert [c for c, _, _ in got] == [0, native.E_SIGNAL, native.E_SIGNAL, 0]
+    assert got[0][1]["moslqo"] == got[3][1]["moslqo"]
+    with pytest.raises(native.NativeError) as e:
+        audio_ctx.measure(np.zeros(100), np.zeros(100), 48000)
+    assert e.value.code == native.E_SIGNAL
+    (code, _, _), = run(audio_ctx, [good], 0)
+    assert code == native.E_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("flags", [dict(disable_global_alignment=True), dict(disable_realignment=True),
+                                   dict(search_window_radius=2)])
+def test_options(native, oracle, flags):
+    from akvisqol_b200 import synth
+    ref, deg = synth.audio_pair(synth.SEED_BASE + 11, seconds=5.0)
+    ctx = native.Context(**flags)
+    (code, res, tr), = ctx.measure_batch_traced([ref], [deg], 48000)
+    o = oracle.options(radius=flags.get("search_window_radius", 60),
+                       disable_global_alignment=flags.get("disable_global_alignment", False),
+                       disable_realignment=flags.get("disable_realignment", False))
+    want, wtr = oracle.measure(ref, deg, 48000, o)
+    assert code == 0
+    assert_same(res, tr, want, wtr)
+
+
+def test_device_resident_inputs(native, oracle, audio_ctx):
+    torch = pytest.importorskip("torch")
+    from akvisqol_b200 import synth
+    pairs = [synth.audio_pair(synth.SEED_BASE + i, seconds=3.5) for i in range(2)]
+    dref = [torch.from_numpy(r).cuda() for r, _ in pairs]
+    ddeg = [torch.from_numpy(d).cuda() for _, d in pairs]
+    torch.cuda.synchronize()
+    got = audio_ctx.measure_batch_traced([t.data_ptr() for t in dref], [t.data_ptr() for t in ddeg], 48000,
+                                         device_inputs=True, ref_lens=[t.numel() for t in dref],
+                                         deg_lens=[t.numel() for t in ddeg])
+    host = run(audio_ctx, pairs, 48000)
+    for (c1, r1, t1), (c2, r2, t2) in zip(got, host):
+        assert c1 == c2 == 0 and r1["moslqo"] == r2["moslqo"]
+
+
+def test_timing_counters(native, audio_ctx):
+    from akvisqol_b200 import synth
+    pairs = [synth.audio_pair(synth.SEED_BASE + i, seconds=3.0) for i in range(2)]
+    run(audio_ctx, pairs, 48000)
+    t = audio_ctx.last_timing()
+    assert t["total_ms"] > 0 and t["gammatone_kernel_ms"] > 0
+    assert t["gammatone_launches"] >= 1 and t["kernel_launches"] > 10
+    assert t["gammatone_window"] == 3840
