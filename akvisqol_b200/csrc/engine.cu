@@ -112,6 +112,9 @@ Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> 
     max_freq_ = opt.speech ? 8000.0 : -1.0;
     VQB_CUDA(cudaSetDevice(device_));
     VQB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    VQB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    VQB_CUDA(cudaEventCreateWithFlags(&ev_inputs_, cudaEventDisableTiming));
+    VQB_CUDA(cudaEventCreateWithFlags(&ev_ref_done_, cudaEventDisableTiming));
     events_.resize(8);
     for (auto &e : events_) VQB_CUDA(cudaEventCreate(&e));
     for (auto &e : gt_events_) VQB_CUDA(cudaEventCreate(&e));
@@ -123,6 +126,10 @@ Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> 
 Engine::~Engine() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (side_) cudaStreamSynchronize(side_);
+    if (ev_inputs_) cudaEventDestroy(ev_inputs_);
+    if (ev_ref_done_) cudaEventDestroy(ev_ref_done_);
+    if (side_) cudaStreamDestroy(side_);
     for (auto &kv : rates_) {
         cudaFree(kv.second.d_coeffs);
         cudaFree(kv.second.d_hann);
@@ -371,6 +378,51 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         s.stats = arena_.alloc_n<double>(10);
     }
 
+    auto run_gammatone = [&](const std::vector<SpecJob> &jobs, cudaStream_t st) {
+        if (jobs.empty()) return;
+        SpecJob *d_jobs = upload(jobs);
+        const int F = gammatone_frames_per_cta(nbi);
+        const size_t tsz = gammatone_tile_size();
+        std::vector<char> tiles;
+        int ntiles = 0;
+        uint64_t rms = 0;
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            rms += (uint64_t)jobs[j].nf * NB;
+            for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
+                tiles.resize(tiles.size() + tsz);
+                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+            }
+        }
+        void *d_tiles = upload_bytes(tiles.data(), tiles.size());
+        if (st != stream_) {
+            // job tables were copied on the main stream
+            record(ev_inputs_);
+            VQB_CUDA(cudaStreamWaitEvent(st, ev_inputs_, 0));
+        }
+        const size_t slot = 2 * timing_.gammatone_launches;
+        VQB_CUDA(cudaEventRecord(gt_events_[slot], st));
+        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
+        VQB_CUDA(cudaEventRecord(gt_events_[slot + 1], st));
+        timing_.gammatone_launches += 1;
+        timing_.gammatone_rms += rms;
+        timing_.gammatone_window = W;
+    };
+
+    // Reference spectrograms need only the reference signal: they run on a
+    // side stream while the main stream does the serial lag-phase work.
+    {
+        std::vector<SpecJob> ref_jobs;
+        for (size_t i = 0; i < n; ++i) {
+            PairState &s = ps[i];
+            if (!s.live || s.rl <= W) continue;
+            s.nf_ref = host::num_frames(s.rl, W, H);
+            s.ref_raw = arena_.alloc_n<double>(NB * s.nf_ref);
+            ref_jobs.push_back(SpecJob{VSig{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, (int64_t)s.nf_ref, s.ref_raw});
+        }
+        run_gammatone(ref_jobs, side_);
+        VQB_CUDA(cudaEventRecord(ev_ref_done_, side_));
+    }
+
     // ---- 1: global lag and SPL energies --------------------------------
     int64_t *d_lags = arena_.alloc_n<int64_t>(n);
     VQB_CUDA(cudaMemsetAsync(d_lags, 0, n * sizeof(int64_t), stream_));
@@ -473,7 +525,6 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         for (size_t p = 0; p < np; ++p) s.width = std::max(s.width, (size_t)s.search.hi[p] + P);
         max_width = std::max(max_width, (int)s.width);
         s.deg_al = arena_.alloc_n<double>((size_t)s.al.len);
-        s.ref_raw = arena_.alloc_n<double>(NB * s.nf_ref);
         s.deg_raw = arena_.alloc_n<double>(NB * s.nf_deg);
         s.ref_prep = arena_.alloc_n<double>(NB * s.nf_ref);
         s.deg_prep = arena_.alloc_n<double>(NB * s.nf_deg);
@@ -495,7 +546,6 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         fill_scale_args(scale_args.data() + scale_args.size() - scale_args_size(), src, s.factor, s.deg_al);
         ++nscale;
         max_al = std::max(max_al, s.al.len);
-        spec_jobs.push_back(SpecJob{VSig{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, (int64_t)s.nf_ref, s.ref_raw});
         spec_jobs.push_back(SpecJob{VSig{s.deg_al, 0, s.al.len, s.al.len}, (int64_t)s.nf_deg, s.deg_raw});
         s.trace.n_rms += NB * (s.nf_ref + s.nf_deg);
         prep_jobs.push_back(PrepJob{s.ref_raw, s.deg_raw, s.ref_prep, s.deg_prep, (int32_t)s.nf_ref, (int32_t)s.nf_deg});
@@ -524,34 +574,11 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     }
 
     // ---- 3: spectrograms, prep, NSIM table, DP, match statistics ----------
-    auto run_gammatone = [&](const std::vector<SpecJob> &jobs) {
-        if (jobs.empty()) return;
-        SpecJob *d_jobs = upload(jobs);
-        const int F = gammatone_frames_per_cta(nbi);
-        const size_t tsz = gammatone_tile_size();
-        std::vector<char> tiles;
-        int ntiles = 0;
-        uint64_t rms = 0;
-        for (size_t j = 0; j < jobs.size(); ++j) {
-            rms += (uint64_t)jobs[j].nf * NB;
-            for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
-                tiles.resize(tiles.size() + tsz);
-                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
-            }
-        }
-        void *d_tiles = upload_bytes(tiles.data(), tiles.size());
-        const size_t slot = 2 * timing_.gammatone_launches;
-        record(gt_events_[slot]);
-        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, stream_);
-        record(gt_events_[slot + 1]);
-        timing_.gammatone_launches += 1;
-        timing_.gammatone_rms += rms;
-        timing_.gammatone_window = W;
-    };
     if (nscale) launch_scale(upload_bytes(scale_args.data(), scale_args.size()), nscale, max_al, stream_);
     record(events_[2]);
-    run_gammatone(spec_jobs);
+    run_gammatone(spec_jobs, stream_);
     record(events_[3]);
+    VQB_CUDA(cudaStreamWaitEvent(stream_, ev_ref_done_, 0));
     if (!prep_jobs.empty()) launch_prep(upload(prep_jobs), (int)prep_jobs.size(), nbi, stream_);
     record(events_[4]);
     if (!plane_jobs.empty()) launch_plane(upload(plane_jobs), (int)plane_jobs.size(), nbi, max_width, stream_);
@@ -709,7 +736,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         }
         // ---- 7: realigned spectrograms and statistics ------------------------
         if (!copies.empty()) launch_copy_frames(upload(copies), (int)copies.size(), nbi, max_cols, stream_);
-        run_gammatone(rjobs);
+        run_gammatone(rjobs, stream_);
         if (!rprep.empty()) launch_prep(upload(rprep), (int)rprep.size(), nbi, stream_);
         if (!rstats.empty()) launch_stats(upload(rstats), (int)rstats.size(), nbi, stream_);
         std::vector<double *> h_rst;

@@ -142,7 +142,9 @@ private:
     std::map<uint32_t, RateCache> rates_;
     std::map<size_t, double2 *> twiddles_;
     std::vector<cudaEvent_t> events_;
-    cudaEvent_t gt_events_[4] = {};  // begin/end of up to two gammatone launches
+    cudaStream_t side_ = nullptr;    // reference spectrograms, concurrent with the lag phase
+    cudaEvent_t ev_inputs_ = nullptr, ev_ref_done_ = nullptr;
+    cudaEvent_t gt_events_[6] = {};  // begin/end of up to three gammatone launches
     Timing timing_;
 };
 

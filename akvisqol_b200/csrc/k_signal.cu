@@ -23,6 +23,65 @@ enum SumKind : int {
     kEnergy = 2,        // out[2] = sum x*x
 };
 
+// Samples in flight per lane: a warp keeps 32 * kDepth samples loaded ahead
+// of the add chain, enough to cover HBM latency with the chain's own time.
+constexpr int kDepth = 8;
+
+// Left-to-right sums, in index order, of KIND's per-sample terms over
+// sample(start + k), k in [0, n). acc0/acc1 are the two chains.
+template <int KIND>
+__device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, double mean, double &acc0,
+                                   double &acc1) {
+    const int lane = threadIdx.x & 31;
+    double cur[kDepth], nxt[kDepth];
+#pragma unroll
+    for (int r = 0; r < kDepth; ++r) {
+        const int64_t k = r * 32 + lane;
+        cur[r] = k < n ? vsig_at(sig, start + k) : 0.0;
+    }
+    for (int64_t base = 0; base < n; base += 32 * kDepth) {
+        const int64_t next_base = base + 32 * kDepth;
+        if (next_base < n) {
+#pragma unroll
+            for (int r = 0; r < kDepth; ++r) {
+                const int64_t k = next_base + r * 32 + lane;
+                nxt[r] = k < n ? vsig_at(sig, start + k) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kDepth; ++r) {
+            const int64_t k = base + r * 32 + lane;
+            const int64_t left = n - (base + r * 32);
+            if (left <= 0) break;
+            const double v = cur[r];
+            double t0, t1 = 0.0;
+            if (KIND == kSumAndEnergy) {
+                t0 = v;
+                t1 = v * v;
+            } else if (KIND == kNyquist) {
+                const double d = v - mean;
+                t0 = (k & 1) ? -d : d;
+            } else {
+                t0 = v * v;
+            }
+            if (left >= 32) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    acc0 += __shfl_sync(kFull, t0, j);
+                    if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
+                }
+            } else {
+                for (int j = 0; j < (int)left; ++j) {
+                    acc0 += __shfl_sync(kFull, t0, j);
+                    if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kDepth; ++r) cur[r] = nxt[r];
+    }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(128) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -32,37 +91,7 @@ __global__ void __launch_bounds__(128) serial_sum_kernel(const SumJob *__restric
     const int64_t len = job.sig.len;
     const double mean = KIND == kNyquist ? job.out[0] / (double)len : 0.0;
     double acc0 = 0.0, acc1 = 0.0;
-    // Software pipeline: the next chunk's load is in flight while the
-    // current chunk's terms are added.
-    double next = lane < len ? vsig_at(job.sig, lane) : 0.0;
-    for (int64_t base = 0; base < len; base += 32) {
-        const double v = next;
-        const int64_t k = base + lane;
-        if (base + 32 < len) next = (k + 32 < len) ? vsig_at(job.sig, k + 32) : 0.0;
-        double t0, t1 = 0.0;
-        if (KIND == kSumAndEnergy) {
-            t0 = v;
-            t1 = v * v;
-        } else if (KIND == kNyquist) {
-            const double d = v - mean;
-            t0 = (k & 1) ? -d : d;
-        } else {
-            t0 = v * v;
-        }
-        const int64_t left = len - base;
-        if (left >= 32) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                acc0 += __shfl_sync(kFull, t0, j);
-                if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
-            }
-        } else {
-            for (int j = 0; j < (int)left; ++j) {
-                acc0 += __shfl_sync(kFull, t0, j);
-                if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
-            }
-        }
-    }
+    warp_serial<KIND>(job.sig, 0, len, mean, acc0, acc1);
     if (lane == 0) {
         if (KIND == kSumAndEnergy) {
             job.out[0] = acc0;
@@ -104,22 +133,8 @@ __global__ void __launch_bounds__(128) aligned_energy_kernel(const AlignedEnergy
             alen = L + lag;
         }
     }
-    double acc = 0.0;
-    const int64_t n = L - skip;
-    double next = lane < n ? vsig_at(job.deg, skip + lane) : 0.0;
-    for (int64_t base = 0; base < n; base += 32) {
-        const double v = next;
-        const int64_t k = base + lane;
-        if (base + 32 < n) next = (k + 32 < n) ? vsig_at(job.deg, skip + k + 32) : 0.0;
-        const double t = v * v;
-        const int64_t left = n - base;
-        if (left >= 32) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) acc += __shfl_sync(kFull, t, j);
-        } else {
-            for (int j = 0; j < (int)left; ++j) acc += __shfl_sync(kFull, t, j);
-        }
-    }
+    double acc = 0.0, unused = 0.0;
+    warp_serial<kEnergy>(job.deg, skip, L - skip, 0.0, acc, unused);
     if (lane == 0) {
         job.out[0] = acc;
         job.out[1] = (double)alen;
