@@ -134,7 +134,7 @@ Engine::~Engine() {
         cudaFree(kv.second.d_coeffs);
         cudaFree(kv.second.d_hann);
     }
-    for (auto &kv : twiddles_) cudaFree(kv.second);
+    for (auto &kv : twiddles_) cudaFree(const_cast<double2 *>(kv.second.top));
     for (auto e : events_) cudaEventDestroy(e);
     for (auto e : gt_events_)
         if (e) cudaEventDestroy(e);
@@ -155,15 +155,19 @@ const Engine::RateCache &Engine::rate_cache(uint32_t sr) {
     return rates_.emplace(sr, std::move(rc)).first->second;
 }
 
-const double2 *Engine::twiddles(size_t n) {
+Engine::Twiddles Engine::twiddles(size_t n) {
     auto it = twiddles_.find(n);
     if (it != twiddles_.end()) return it->second;
-    const std::vector<double2> t = host::twiddles(n);
+    // top[k] = W_n^k (k < n/2), then the block passes' W_B^k = top[k * n/B].
+    std::vector<double2> t = host::twiddles(n);
+    const size_t B = (size_t)fft_block_size((int64_t)n), half = t.size();
+    for (size_t k = 0; k < B / 2; ++k) t.push_back(t[k * (n / B)]);
     double2 *d = nullptr;
     VQB_CUDA(cudaMalloc(&d, std::max<size_t>(1, t.size()) * sizeof(double2)));
     if (!t.empty()) VQB_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
-    twiddles_[n] = d;
-    return d;
+    Twiddles tw{d, d + half};
+    twiddles_[n] = tw;
+    return tw;
 }
 
 template <class T>
@@ -208,7 +212,7 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
     const size_t budget = size_t(4) << 30;
     for (auto &g : groups) {
         const int64_t n = g.first;
-        const double2 *top = twiddles((size_t)n);
+        const Twiddles tw = twiddles((size_t)n);
         const size_t per = std::max<size_t>(1, budget / ((size_t)n * sizeof(double2)));
         for (size_t c0 = 0; c0 < g.second.size(); c0 += per) {
             const size_t cnt = std::min(per, g.second.size() - c0);
@@ -223,9 +227,9 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
             double *pv = arena_.alloc_n<double>((size_t)parts * cnt);
             int64_t *pk = arena_.alloc_n<int64_t>((size_t)parts * cnt);
             launch_pack(d_jobs, (int)cnt, n, raw, stream_);
-            launch_fft(z, n, false, top, (int)cnt, n, stream_);
+            launch_fft(z, n, false, tw.top, tw.block, (int)cnt, n, stream_);
             launch_cross(z, n, (int)cnt, n, stream_);
-            launch_fft(z, n, true, top, (int)cnt, n, stream_);
+            launch_fft(z, n, true, tw.top, tw.block, (int)cnt, n, stream_);
             launch_argmax(z, d_jobs, (int)cnt, n, n, pv, pk, stream_);
         }
     }

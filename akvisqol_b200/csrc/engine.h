@@ -109,7 +109,12 @@ public:
     void spectrogram(const host::Filterbank &fb, const double *d_hann, size_t window, size_t hop, const double *d_x,
                      size_t len, double *d_out, size_t nf);
     void lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags);
-    const double2 *twiddles(size_t n);
+    // FFT twiddles of size n on the device: the full table and the block
+    // passes' compact one (cached per size).
+    struct Twiddles {
+        const double2 *top, *block;
+    };
+    Twiddles twiddles(size_t n);
 
 private:
     struct RateCache {
@@ -140,7 +145,7 @@ private:
     Arena arena_;
     PinnedArena pinned_;
     std::map<uint32_t, RateCache> rates_;
-    std::map<size_t, double2 *> twiddles_;
+    std::map<size_t, Twiddles> twiddles_;
     std::vector<cudaEvent_t> events_;
     cudaStream_t side_ = nullptr;    // reference spectrograms, concurrent with the lag phase
     cudaEvent_t ev_inputs_ = nullptr, ev_ref_done_ = nullptr;

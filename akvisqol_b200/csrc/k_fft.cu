@@ -84,40 +84,107 @@ __global__ void __launch_bounds__(128) global_pass(double2 *__restrict__ z, int6
 }
 
 // All stages with span <= B of each B-point block (B = min(n, 4096)) in
-// shared memory.
+// shared memory, two stages per barrier (radix 4) with a radix-2 stage
+// where the stage count is odd. tw[k] = W_B^k (k < B/2), so the span-s
+// twiddle W_s^j is tw[j * B/s]: the same values as the full table.
+__device__ inline void dif2(double2 *sm, int B, int s, const double2 *tw) {
+    const int h = s >> 1, step = B / s;
+    for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
+        const int blk = bf / h, j = bf - blk * h;
+        const int i0 = blk * s + j;
+        const double2 a = sm[i0], b = sm[i0 + h];
+        sm[i0] = cadd(a, b);
+        sm[i0 + h] = cmul(csub(a, b), tw[j * step]);
+    }
+}
+__device__ inline void dit2(double2 *sm, int B, int s, const double2 *tw) {
+    const int h = s >> 1, step = B / s;
+    for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
+        const int blk = bf / h, j = bf - blk * h;
+        const int i0 = blk * s + j;
+        const double2 a = sm[i0];
+        const double2 b = cmul_conj(sm[i0 + h], tw[j * step]);
+        sm[i0] = cadd(a, b);
+        sm[i0 + h] = csub(a, b);
+    }
+}
+// Spans s then s/2 on 4-point groups spaced q = s/4 apart.
+__device__ inline void dif4(double2 *sm, int B, int s, const double2 *tw) {
+    const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
+    for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
+        const int blk = g / q, j = g - blk * q;
+        const int b0 = blk * s + j;
+        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        double2 a = x0, b = x2;
+        x0 = cadd(a, b);
+        x2 = cmul(csub(a, b), tw[j * st1]);
+        a = x1, b = x3;
+        x1 = cadd(a, b);
+        x3 = cmul(csub(a, b), tw[(j + q) * st1]);
+        const double2 w = tw[j * st2];
+        a = x0, b = x1;
+        x0 = cadd(a, b);
+        x1 = cmul(csub(a, b), w);
+        a = x2, b = x3;
+        x2 = cadd(a, b);
+        x3 = cmul(csub(a, b), w);
+        sm[b0] = x0, sm[b0 + q] = x1, sm[b0 + 2 * q] = x2, sm[b0 + 3 * q] = x3;
+    }
+}
+// Spans s/2 then s.
+__device__ inline void dit4(double2 *sm, int B, int s, const double2 *tw) {
+    const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
+    for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
+        const int blk = g / q, j = g - blk * q;
+        const int b0 = blk * s + j;
+        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        const double2 w = tw[j * st2];
+        double2 a = x0, b = cmul_conj(x1, w);
+        x0 = cadd(a, b);
+        x1 = csub(a, b);
+        a = x2, b = cmul_conj(x3, w);
+        x2 = cadd(a, b);
+        x3 = csub(a, b);
+        a = x0, b = cmul_conj(x2, tw[j * st1]);
+        x0 = cadd(a, b);
+        x2 = csub(a, b);
+        a = x1, b = cmul_conj(x3, tw[(j + q) * st1]);
+        x1 = cadd(a, b);
+        x3 = csub(a, b);
+        sm[b0] = x0, sm[b0 + q] = x1, sm[b0 + 2 * q] = x2, sm[b0 + 3 * q] = x3;
+    }
+}
+
 template <bool DIT>
-__global__ void __launch_bounds__(256) block_pass(double2 *__restrict__ z, int64_t n, int B,
-                                                  const double2 *__restrict__ top, int64_t job_stride) {
+__global__ void __launch_bounds__(256) block_pass(double2 *__restrict__ z, int B, const double2 *__restrict__ tw,
+                                                  int64_t job_stride) {
     extern __shared__ double2 sm[];
     double2 *zz = z + (int64_t)blockIdx.y * job_stride + (int64_t)blockIdx.x * B;
     for (int i = threadIdx.x; i < B; i += blockDim.x) sm[i] = zz[i];
     __syncthreads();
-    const int half = B >> 1;
+    int stages = 0;
+    for (int r = B; r > 1; r >>= 1) ++stages;
     if (!DIT) {
-        for (int s = B; s >= 2; s >>= 1) {
-            const int h = s >> 1;
-            const int64_t stride = n / s;
-            for (int bf = threadIdx.x; bf < half; bf += blockDim.x) {
-                const int blk = bf / h, j = bf - blk * h;
-                const int i0 = blk * s + j;
-                const double2 a = sm[i0], b = sm[i0 + h];
-                sm[i0] = cadd(a, b);
-                sm[i0 + h] = cmul(csub(a, b), top[j * stride]);
-            }
+        int s = B;
+        for (; stages >= 2; stages -= 2, s >>= 2) {
+            dif4(sm, B, s, tw);
+            __syncthreads();
+        }
+        if (stages == 1) {
+            dif2(sm, B, 2, tw);
             __syncthreads();
         }
     } else {
-        for (int s = 2; s <= B; s <<= 1) {
-            const int h = s >> 1;
-            const int64_t stride = n / s;
-            for (int bf = threadIdx.x; bf < half; bf += blockDim.x) {
-                const int blk = bf / h, j = bf - blk * h;
-                const int i0 = blk * s + j;
-                const double2 a = sm[i0];
-                const double2 b = cmul_conj(sm[i0 + h], top[j * stride]);
-                sm[i0] = cadd(a, b);
-                sm[i0 + h] = csub(a, b);
-            }
+        int s = 2;
+        if (stages & 1) {
+            dit2(sm, B, 2, tw);
+            __syncthreads();
+            s = 8;
+        } else {
+            s = 4;
+        }
+        for (; s <= B; s <<= 2) {
+            dit4(sm, B, s, tw);
             __syncthreads();
         }
     }
@@ -204,7 +271,6 @@ __global__ void argmax_final(const LagJob *__restrict__ jobs, int njobs, const d
     *jobs[j].lag_out = best.key == INT64_MAX ? 0 : best.key - max_lag;
 }
 
-template <bool DIT>
 void global_passes_dif(double2 *z, int64_t n, int64_t block, const double2 *top, int njobs, int64_t stride,
                        cudaStream_t s) {
     // DIF: spans n down to block*2, up to 4 stages per pass.
@@ -248,32 +314,36 @@ void global_passes_dit(double2 *z, int64_t n, int64_t block, const double2 *top,
 
 constexpr int kBlock = 4096;
 
-void block_passes(double2 *z, int64_t n, bool dit, const double2 *top, int njobs, int64_t stride, cudaStream_t s) {
+void block_passes(double2 *z, int64_t n, bool dit, const double2 *tw_block, int njobs, int64_t stride,
+                  cudaStream_t s) {
     const int B = (int)(n < kBlock ? n : kBlock);
     if (B < 2) return;
     const size_t smem = (size_t)B * sizeof(double2);
     dim3 grid((unsigned)(n / B), (unsigned)njobs);
     if (dit)
-        block_pass<true><<<grid, 256, smem, s>>>(z, n, B, top, stride);
+        block_pass<true><<<grid, 256, smem, s>>>(z, B, tw_block, stride);
     else
-        block_pass<false><<<grid, 256, smem, s>>>(z, n, B, top, stride);
+        block_pass<false><<<grid, 256, smem, s>>>(z, B, tw_block, stride);
     launch_counter() += 1;
 }
 
 }  // namespace
+
+int fft_block_size(int64_t n) { return (int)(n < kBlock ? n : kBlock); }
 
 void fft_init_attributes() {
     cudaFuncSetAttribute(block_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlock * (int)sizeof(double2));
     cudaFuncSetAttribute(block_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlock * (int)sizeof(double2));
 }
 
-void launch_fft(double2 *z, int64_t n, bool inverse, const double2 *top, int njobs, int64_t stride, cudaStream_t s) {
+void launch_fft(double2 *z, int64_t n, bool inverse, const double2 *top, const double2 *tw_block, int njobs,
+                int64_t stride, cudaStream_t s) {
     const int64_t block = n < kBlock ? n : kBlock;
     if (!inverse) {
-        global_passes_dif<false>(z, n, block, top, njobs, stride, s);
-        block_passes(z, n, false, top, njobs, stride, s);
+        global_passes_dif(z, n, block, top, njobs, stride, s);
+        block_passes(z, n, false, tw_block, njobs, stride, s);
     } else {
-        block_passes(z, n, true, top, njobs, stride, s);
+        block_passes(z, n, true, tw_block, njobs, stride, s);
         global_passes_dit(z, n, block, top, njobs, stride, s);
     }
 }

@@ -4,10 +4,10 @@
 // The reference sums signals left to right in f64 (envelope mean and
 // Nyquist term, src/envelope.zig:28-41; SPL energy, src/audio.zig:132-136).
 // A parallel tree would round differently, so each reduction runs as one
-// warp per signal: the warp loads 32 consecutive samples (one coalesced
-// 256-byte read), forms the per-sample terms in parallel, and every lane
-// then adds the 32 terms in index order from register shuffles. The add
-// chain is the only serial part; many signals run side by side.
+// warp per signal: the warp loads tiles of consecutive samples (coalesced),
+// forms the per-sample terms in parallel into shared memory, and then adds
+// them in index order. The f64 add chain is the only serial part; many
+// signals run side by side.
 #include "device.cuh"
 #include "kernels.h"
 
@@ -15,75 +15,90 @@ namespace vqb {
 
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
-
 enum SumKind : int {
     kSumAndEnergy = 0,  // out[0] = sum x, out[2] = sum x*x
     kNyquist = 1,       // out[1] = sum (-1)^k (x - out[0]/len); reads out[0]
     kEnergy = 2,        // out[2] = sum x*x
 };
 
-// Samples in flight per lane: a warp keeps 32 * kDepth samples loaded ahead
-// of the add chain, enough to cover HBM latency with the chain's own time.
-constexpr int kDepth = 8;
+// Samples per tile: each lane loads 8 (coalesced 256-byte rows), forms the
+// per-sample terms, and writes them to this warp's shared-memory tile;
+// then every lane walks the tile in index order adding broadcast reads, so
+// the only serial dependency left is the f64 add itself. The next tile's
+// global loads are in flight meanwhile (double buffering).
+constexpr int kRows = 8;
+constexpr int kTile = 32 * kRows;
+constexpr int kSerialWarps = 4;
+
+template <int KIND>
+__device__ inline void tile_terms(double v, int64_t k, double mean, double &t0, double &t1) {
+    if (KIND == kSumAndEnergy) {
+        t0 = v;
+        t1 = v * v;
+    } else if (KIND == kNyquist) {
+        const double d = v - mean;
+        t0 = (k & 1) ? -d : d;
+    } else {
+        t0 = v * v;
+    }
+}
 
 // Left-to-right sums, in index order, of KIND's per-sample terms over
-// sample(start + k), k in [0, n). acc0/acc1 are the two chains.
+// sample(start + k), k in [0, n): chain 0 (and chain 1 for kSumAndEnergy).
+// tiles: this warp's 2 (buffers) x 2 (chains) x kTile doubles.
 template <int KIND>
 __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, double mean, double &acc0,
-                                   double &acc1) {
+                                   double &acc1, double *tiles) {
     const int lane = threadIdx.x & 31;
-    double cur[kDepth], nxt[kDepth];
+    double reg[kRows];
+    auto load = [&](int64_t base) {
 #pragma unroll
-    for (int r = 0; r < kDepth; ++r) {
-        const int64_t k = r * 32 + lane;
-        cur[r] = k < n ? vsig_at(sig, start + k) : 0.0;
-    }
-    for (int64_t base = 0; base < n; base += 32 * kDepth) {
-        const int64_t next_base = base + 32 * kDepth;
-        if (next_base < n) {
-#pragma unroll
-            for (int r = 0; r < kDepth; ++r) {
-                const int64_t k = next_base + r * 32 + lane;
-                nxt[r] = k < n ? vsig_at(sig, start + k) : 0.0;
-            }
-        }
-#pragma unroll
-        for (int r = 0; r < kDepth; ++r) {
+        for (int r = 0; r < kRows; ++r) {
             const int64_t k = base + r * 32 + lane;
-            const int64_t left = n - (base + r * 32);
-            if (left <= 0) break;
-            const double v = cur[r];
-            double t0, t1 = 0.0;
-            if (KIND == kSumAndEnergy) {
-                t0 = v;
-                t1 = v * v;
-            } else if (KIND == kNyquist) {
-                const double d = v - mean;
-                t0 = (k & 1) ? -d : d;
-            } else {
-                t0 = v * v;
-            }
-            if (left >= 32) {
+            reg[r] = k < n ? vsig_at(sig, start + k) : 0.0;
+        }
+    };
+    auto store = [&](int64_t base, int buf) {
+        double *c0 = tiles + buf * 2 * kTile, *c1 = c0 + kTile;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    acc0 += __shfl_sync(kFull, t0, j);
-                    if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
-                }
-            } else {
-                for (int j = 0; j < (int)left; ++j) {
-                    acc0 += __shfl_sync(kFull, t0, j);
-                    if (KIND == kSumAndEnergy) acc1 += __shfl_sync(kFull, t1, j);
-                }
+        for (int r = 0; r < kRows; ++r) {
+            double t0, t1 = 0.0;
+            tile_terms<KIND>(reg[r], base + r * 32 + lane, mean, t0, t1);
+            c0[r * 32 + lane] = t0;
+            if (KIND == kSumAndEnergy) c1[r * 32 + lane] = t1;
+        }
+    };
+    if (n <= 0) return;
+    load(0);
+    store(0, 0);
+    __syncwarp();
+    int buf = 0;
+    for (int64_t base = 0; base < n; base += kTile) {
+        const int64_t next = base + kTile;
+        if (next < n) load(next);
+        const double *c0 = tiles + buf * 2 * kTile, *c1 = c0 + kTile;
+        const int64_t left = n - base;
+        if (left >= kTile) {
+#pragma unroll 32
+            for (int e = 0; e < kTile; ++e) {
+                acc0 += c0[e];
+                if (KIND == kSumAndEnergy) acc1 += c1[e];
+            }
+        } else {
+            for (int e = 0; e < (int)left; ++e) {
+                acc0 += c0[e];
+                if (KIND == kSumAndEnergy) acc1 += c1[e];
             }
         }
-#pragma unroll
-        for (int r = 0; r < kDepth; ++r) cur[r] = nxt[r];
+        if (next < n) store(next, buf ^ 1);
+        __syncwarp();
+        buf ^= 1;
     }
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(128) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
+__global__ void __launch_bounds__(32 * kSerialWarps) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
+    __shared__ double tiles[kSerialWarps][4 * kTile];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -91,7 +106,7 @@ __global__ void __launch_bounds__(128) serial_sum_kernel(const SumJob *__restric
     const int64_t len = job.sig.len;
     const double mean = KIND == kNyquist ? job.out[0] / (double)len : 0.0;
     double acc0 = 0.0, acc1 = 0.0;
-    warp_serial<KIND>(job.sig, 0, len, mean, acc0, acc1);
+    warp_serial<KIND>(job.sig, 0, len, mean, acc0, acc1, tiles[threadIdx.x >> 5]);
     if (lane == 0) {
         if (KIND == kSumAndEnergy) {
             job.out[0] = acc0;
@@ -115,7 +130,9 @@ struct AlignedEnergyArgs {
     double *out;  // [energy, aligned length]
 };
 
-__global__ void __launch_bounds__(128) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs, int njobs) {
+__global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs,
+                                                                            int njobs) {
+    __shared__ double tiles[kSerialWarps][4 * kTile];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -134,7 +151,7 @@ __global__ void __launch_bounds__(128) aligned_energy_kernel(const AlignedEnergy
         }
     }
     double acc = 0.0, unused = 0.0;
-    warp_serial<kEnergy>(job.deg, skip, L - skip, 0.0, acc, unused);
+    warp_serial<kEnergy>(job.deg, skip, L - skip, 0.0, acc, unused, tiles[threadIdx.x >> 5]);
     if (lane == 0) {
         job.out[0] = acc;
         job.out[1] = (double)alen;

@@ -61,7 +61,11 @@ void launch_scale(const void *d_args, int njobs, int64_t max_len, cudaStream_t s
 
 // k_fft.cu
 void fft_init_attributes();
-void launch_fft(double2 *z, int64_t n, bool inverse, const double2 *top, int njobs, int64_t stride, cudaStream_t s);
+// Block size of the shared-memory passes, min(n, 4096); tw_block[k] =
+// W_B^k = top[k * n/B] for k < B/2.
+int fft_block_size(int64_t n);
+void launch_fft(double2 *z, int64_t n, bool inverse, const double2 *top, const double2 *tw_block, int njobs,
+                int64_t stride, cudaStream_t s);
 void launch_cross(double2 *z, int64_t n, int njobs, int64_t stride, cudaStream_t s);
 int argmax_parts(int64_t n);
 void launch_argmax(const double2 *z, const LagJob *d_jobs, int njobs, int64_t n, int64_t stride, double *pv,

@@ -108,7 +108,8 @@ int visqol_b200_fft(double *buf, size_t n, int inverse) {
     return guarded([&] {
         vqb::Engine &e = stage_engine();
         DBuf<double2> z(reinterpret_cast<const double2 *>(buf), n);
-        vqb::launch_fft(z.p, (int64_t)n, inverse != 0, e.twiddles(n), 1, (int64_t)n, e.stream());
+        const auto tw = e.twiddles(n);
+        vqb::launch_fft(z.p, (int64_t)n, inverse != 0, tw.top, tw.block, 1, (int64_t)n, e.stream());
         VQB_CUDA(cudaStreamSynchronize(e.stream()));
         z.get(reinterpret_cast<double2 *>(buf), n);
     });
