@@ -5,12 +5,15 @@
 // per-pair status in batches (the first error is the return value), and
 // files grouped by sample rate. The engine behind it is the GPU pipeline;
 // there is no CPU fallback.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -22,10 +25,16 @@
 
 using vqb::Error;
 
+// A context owns one or more lanes: engines with their own streams and
+// memory on the same GPU (VISQOL_GPU_LANES, default 2, as the reference's
+// GPU engine, src/gpu/engine.zig:551-591). A batch is split across the
+// lanes by signal length and the lanes run concurrently from host threads,
+// so one lane's serial phases and host planning overlap another's kernels.
 struct visqol_ctx {
     vqb::Options opt;
     std::shared_ptr<const vqb::host::Svr> svr;
-    std::unique_ptr<vqb::Engine> engine;
+    std::vector<std::unique_ptr<vqb::Engine>> lanes;
+    vqb::Timing timing;
 };
 
 namespace {
@@ -116,13 +125,80 @@ int device_count() {
     return n;
 }
 
+// The batch across the context's lanes: pairs dealt longest-first to the
+// least-loaded lane, lanes run concurrently, outcomes gathered back in order.
+void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
+               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, std::vector<vqb::PairOutcome> &res) {
+    const size_t L = std::min(c->lanes.size(), std::max<size_t>(1, n));
+    res.assign(n, vqb::PairOutcome{});
+    if (L <= 1) {
+        c->lanes[0]->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
+        c->timing = c->lanes[0]->last_timing();
+        return;
+    }
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return ref_lens[a] + deg_lens[a] > ref_lens[b] + deg_lens[b];
+    });
+    std::vector<std::vector<size_t>> part(L);
+    std::vector<size_t> load(L, 0);
+    for (size_t i : order) {
+        const size_t l = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        part[l].push_back(i);
+        load[l] += ref_lens[i] + deg_lens[i];
+    }
+    std::vector<std::vector<vqb::PairOutcome>> lane_out(L);
+    std::vector<std::exception_ptr> errs(L);
+    auto work = [&](size_t l) {
+        try {
+            const auto &ix = part[l];
+            std::vector<const double *> r(ix.size()), d(ix.size());
+            std::vector<size_t> rl(ix.size()), dl(ix.size());
+            for (size_t k = 0; k < ix.size(); ++k)
+                r[k] = refs[ix[k]], d[k] = degs[ix[k]], rl[k] = ref_lens[ix[k]], dl[k] = deg_lens[ix[k]];
+            c->lanes[l]->measure_batch(ix.size(), r.data(), rl.data(), d.data(), dl.data(), sample_rate, device_inputs,
+                                       lane_out[l]);
+        } catch (...) {
+            errs[l] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> threads;
+    for (size_t l = 1; l < L; ++l) threads.emplace_back(work, l);
+    work(0);
+    for (auto &t : threads) t.join();
+    for (auto &e : errs)
+        if (e) std::rethrow_exception(e);
+    vqb::Timing t{};
+    for (size_t l = 0; l < L; ++l) {
+        for (size_t k = 0; k < part[l].size(); ++k) res[part[l][k]] = std::move(lane_out[l][k]);
+        const vqb::Timing &x = c->lanes[l]->last_timing();
+        // lanes overlap: spans are the longest lane's, work counts add up
+        t.total_ms = std::max(t.total_ms, x.total_ms);
+        t.lag_ms = std::max(t.lag_ms, x.lag_ms);
+        t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
+        t.prep_ms = std::max(t.prep_ms, x.prep_ms);
+        t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
+        t.realign_ms = std::max(t.realign_ms, x.realign_ms);
+        t.gammatone_kernel_ms += x.gammatone_kernel_ms;
+        t.gammatone_launches += x.gammatone_launches;
+        t.gammatone_rms += x.gammatone_rms;
+        t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
+        t.kernel_launches += x.kernel_launches;
+        t.h2d_bytes += x.h2d_bytes;
+        t.d2h_bytes += x.d2h_bytes;
+        t.host_syncs += x.host_syncs;
+    }
+    c->timing = t;
+}
+
 // One batch through the engine with per-pair results and status.
 int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, visqol_result **out, int32_t *status,
               visqol_b200_trace **traces) {
     std::vector<vqb::PairOutcome> res;
     try {
-        c->engine->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
+        run_lanes(c, n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
     } catch (const Error &e) {
         for (size_t i = 0; i < n; ++i) {
             out[i] = nullptr;
@@ -221,7 +297,10 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
         int dev = 0;
         if (const char *env = std::getenv("VISQOL_CUDA_DEVICE")) dev = std::atoi(env);
         if (dev < 0 || dev >= ndev) return fail(VISQOL_E_INVALID_ARGUMENT, "VISQOL_CUDA_DEVICE out of range");
-        c->engine = std::make_unique<vqb::Engine>(dev, c->opt, c->svr);
+        int lanes = 2;
+        if (const char *env = std::getenv("VISQOL_GPU_LANES")) lanes = std::atoi(env);
+        lanes = std::max(1, std::min(lanes, 8));
+        for (int l = 0; l < lanes; ++l) c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr));
     } catch (const Error &e) {
         return fail(e.code, e.what());
     } catch (const std::bad_alloc &) {
@@ -367,7 +446,7 @@ void visqol_b200_trace_free(visqol_b200_trace *t) {
 
 int visqol_b200_last_timing(visqol_ctx *c, visqol_b200_timing *out) {
     if (!c || !out) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
-    const vqb::Timing &t = c->engine->last_timing();
+    const vqb::Timing &t = c->timing;
     out->total_ms = t.total_ms;
     out->lag_ms = t.lag_ms;
     out->spectrogram_ms = t.spectrogram_ms;

@@ -111,14 +111,20 @@ Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> 
     patch_ = opt.speech ? 20 : 30;
     max_freq_ = opt.speech ? 8000.0 : -1.0;
     VQB_CUDA(cudaSetDevice(device_));
-    VQB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    VQB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    // The main stream carries the latency-critical chain (serial sums, FFTs,
+    // read-backs): highest priority, so its CTAs take SMs first as the side
+    // stream's long gammatone grid drains.
+    int lo_prio = 0, hi_prio = 0;
+    VQB_CUDA(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
+    VQB_CUDA(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, hi_prio));
+    VQB_CUDA(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, lo_prio));
     VQB_CUDA(cudaEventCreateWithFlags(&ev_inputs_, cudaEventDisableTiming));
     VQB_CUDA(cudaEventCreateWithFlags(&ev_ref_done_, cudaEventDisableTiming));
     events_.resize(8);
     for (auto &e : events_) VQB_CUDA(cudaEventCreate(&e));
     for (auto &e : gt_events_) VQB_CUDA(cudaEventCreate(&e));
     fft_init_attributes();
+    lag_init_attributes();
     nsim_init_attributes();
     VQB_CUDA(cudaGetLastError());
 }
@@ -223,6 +229,13 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
                 chunk[k].z = z + (int64_t)k * n;
             }
             LagJob *d_jobs = upload(chunk);
+            if (fused_lag_supported(n)) {
+                const size_t parts = fused_lag_parts(n);
+                double *pv = arena_.alloc_n<double>(parts * cnt);
+                int64_t *pk = arena_.alloc_n<int64_t>(parts * cnt);
+                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.top, tw.block, pv, pk, stream_);
+                continue;
+            }
             const int parts = argmax_parts(n);
             double *pv = arena_.alloc_n<double>((size_t)parts * cnt);
             int64_t *pk = arena_.alloc_n<int64_t>((size_t)parts * cnt);

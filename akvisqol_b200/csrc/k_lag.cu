@@ -1,0 +1,457 @@
+// Fused FFT cross-correlation lag search (reference src/xcorr.zig:197-251),
+// three passes over the n-point complex buffer instead of one per stage group:
+//
+//   1. pack + global DIF stages: view the n = R * 4096 points as R rows of
+//      4096 columns. The DIF stages with spans n .. 8192 only combine points
+//      of one column, so a CTA loads `cols` whole columns (R x cols points,
+//      64 KB), forms the envelopes on the fly from the signals, runs those
+//      stages in shared memory and writes z once.
+//   2. block stages + cross spectrum: the remaining DIF stages (spans
+//      4096 .. 2) stay inside 4096-point blocks, and in bit-reversed order a
+//      block's cross-spectrum partners Z[-k] all sit in one mirror block
+//      (position u of block b pairs with 4095 - u of block b'), so a CTA loads
+//      a block and its mirror, finishes the forward transform, forms the
+//      cross terms, and runs the inverse's block stages (spans 2 .. 4096).
+//   3. global DIT stages + argmax: columns again; after the last stage each
+//      CTA reduces |Re| over its lags in the CPU's scan order and writes one
+//      candidate; a final kernel picks the first maximum.
+//
+// Butterflies and twiddles are those of the radix-2 DIF/DIT (reference
+// src/dsp/fft.zig:127-166); every schedule of them gives the same bits.
+#include "device.cuh"
+#include "kernels.h"
+
+namespace vqb {
+
+namespace {
+
+constexpr int kB = 4096;        // block (and column-tile) points
+constexpr int kThreads = 256;
+
+__device__ inline double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ inline double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ inline double2 cmul(double2 x, double2 w) {
+    return make_double2(x.x * w.x - x.y * w.y, x.x * w.y + x.y * w.x);
+}
+__device__ inline double2 cmul_conj(double2 x, double2 w) {
+    const double wi = -w.y;
+    return make_double2(x.x * w.x - x.y * wi, x.x * wi + x.y * w.x);
+}
+__device__ inline double2 cross_term(double2 x, double2 zy) {
+    const double2 y = make_double2(zy.x, -zy.y);
+    const double2 sum = make_double2(x.x + y.x, x.y + y.y);
+    const double2 dif_c = make_double2(x.x - y.x, -(x.y - y.y));
+    const double2 idc = make_double2(-dif_c.y, dif_c.x);
+    return make_double2(0.25 * (sum.x * idc.x - sum.y * idc.y), 0.25 * (sum.x * idc.y + sum.y * idc.x));
+}
+
+__host__ __device__ inline int64_t pow2_at_least(int64_t x) {
+    int64_t n = 1;
+    while (n < x) n <<= 1;
+    return n;
+}
+
+// Envelope parameters of one signal: mean and +-nyquist/N.
+struct EnvParams {
+    double mean, q;
+};
+
+__device__ inline EnvParams env_params(const VSig &s, const double *stats) {
+    EnvParams p{0.0, 0.0};
+    if (s.len > 0) {
+        p.mean = stats[0] / (double)s.len;
+        const int64_t N = pow2_at_least(s.len) > 32 ? pow2_at_least(s.len) : 32;
+        p.q = stats[1] / (double)N;
+    }
+    return p;
+}
+
+// upperEnvelope (reference src/envelope.zig:45-52) at sample i.
+__device__ inline double env_at(const VSig &s, const EnvParams &p, int64_t i) {
+    const double x = vsig_at(s, i);
+    const double pc = x - p.mean;
+    const double nt = (i & 1) ? -p.q : p.q;
+    return fabs(2.0 * (pc - nt) - 0.000001) + p.mean;
+}
+
+template <bool RAW>
+__device__ inline double2 packed(const LagJob &job, const EnvParams &pa, const EnvParams &pb, int64_t i) {
+    double re = 0.0, im = 0.0;
+    if (i < job.a.len) re = RAW ? vsig_at(job.a, i) : env_at(job.a, pa, i);
+    if (i < job.b.len) im = RAW ? vsig_at(job.b, i) : env_at(job.b, pb, i);
+    return make_double2(re, im);
+}
+
+// G column stages on x[t * cols + c] (t < R = 2^G rows); DIT reverses the
+// stage order. Stage l has span n >> l; the twiddle of the lower point (t, c)
+// is W_{n>>l}^j = top[j << l] with j = (t mod 2h) * 4096 + c0 + c.
+template <bool DIT>
+__device__ inline void column_stages(double2 *x, int G, int cols, int64_t c0, const double2 *__restrict__ top) {
+    const int R = 1 << G;
+    const int pairs = (R >> 1) * cols;
+    for (int li = 0; li < G; ++li) {
+        const int l = DIT ? G - 1 - li : li;
+        const int h = R >> (l + 1);
+        for (int bf = threadIdx.x; bf < pairs; bf += blockDim.x) {
+            const int pr = bf / cols, c = bf - pr * cols;
+            const int t = (pr / h) * 2 * h + (pr % h);
+            const int64_t j = (int64_t)(t % (2 * h)) * kB + c0 + c;
+            const double2 w = top[j << l];
+            double2 *pa = x + t * cols + c, *pb = x + (t + h) * cols + c;
+            const double2 a = *pa;
+            if (!DIT) {
+                const double2 b = *pb;
+                *pa = cadd(a, b);
+                *pb = cmul(csub(a, b), w);
+            } else {
+                const double2 b = cmul_conj(*pb, w);
+                *pa = cadd(a, b);
+                *pb = csub(a, b);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 1: pack + DIF column stages. grid (n / (R*cols) ... = 4096/cols, jobs).
+template <bool RAW>
+__global__ void __launch_bounds__(kThreads) fwd_columns(const LagJob *__restrict__ jobs, int G,
+                                                        const double2 *__restrict__ top) {
+    extern __shared__ double2 sm[];
+    const LagJob job = jobs[blockIdx.y];
+    const int R = 1 << G, cols = kB >> G > 0 ? (kB >> G) : 1;
+    const int64_t c0 = (int64_t)blockIdx.x * cols;
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+        const int t = e / cols, c = e - t * cols;
+        sm[e] = packed<RAW>(job, pa, pb, (int64_t)t * kB + c0 + c);
+    }
+    __syncthreads();
+    column_stages<false>(sm, G, cols, c0, top);
+    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+        const int t = e / cols, c = e - t * cols;
+        job.z[(int64_t)t * kB + c0 + c] = sm[e];
+    }
+}
+
+// Radix-4/radix-2 block stages of one B-point block in shared memory
+// (tw[k] = W_B^k); the same stage plans as the stand-alone block passes.
+__device__ inline void dif2(double2 *sm, int B, int s, const double2 *tw) {
+    const int h = s >> 1, step = B / s;
+    for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
+        const int blk = bf / h, j = bf - blk * h;
+        const int i0 = blk * s + j;
+        const double2 a = sm[i0], b = sm[i0 + h];
+        sm[i0] = cadd(a, b);
+        sm[i0 + h] = cmul(csub(a, b), tw[j * step]);
+    }
+}
+__device__ inline void dit2(double2 *sm, int B, int s, const double2 *tw) {
+    const int h = s >> 1, step = B / s;
+    for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
+        const int blk = bf / h, j = bf - blk * h;
+        const int i0 = blk * s + j;
+        const double2 a = sm[i0];
+        const double2 b = cmul_conj(sm[i0 + h], tw[j * step]);
+        sm[i0] = cadd(a, b);
+        sm[i0 + h] = csub(a, b);
+    }
+}
+__device__ inline void dif4(double2 *sm, int B, int s, const double2 *tw) {
+    const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
+    for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
+        const int blk = g / q, j = g - blk * q;
+        const int b0 = blk * s + j;
+        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        double2 a = x0, b = x2;
+        x0 = cadd(a, b);
+        x2 = cmul(csub(a, b), tw[j * st1]);
+        a = x1, b = x3;
+        x1 = cadd(a, b);
+        x3 = cmul(csub(a, b), tw[(j + q) * st1]);
+        const double2 w = tw[j * st2];
+        a = x0, b = x1;
+        x0 = cadd(a, b);
+        x1 = cmul(csub(a, b), w);
+        a = x2, b = x3;
+        x2 = cadd(a, b);
+        x3 = cmul(csub(a, b), w);
+        sm[b0] = x0, sm[b0 + q] = x1, sm[b0 + 2 * q] = x2, sm[b0 + 3 * q] = x3;
+    }
+}
+__device__ inline void dit4(double2 *sm, int B, int s, const double2 *tw) {
+    const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
+    for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
+        const int blk = g / q, j = g - blk * q;
+        const int b0 = blk * s + j;
+        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        const double2 w = tw[j * st2];
+        double2 a = x0, b = cmul_conj(x1, w);
+        x0 = cadd(a, b);
+        x1 = csub(a, b);
+        a = x2, b = cmul_conj(x3, w);
+        x2 = cadd(a, b);
+        x3 = csub(a, b);
+        a = x0, b = cmul_conj(x2, tw[j * st1]);
+        x0 = cadd(a, b);
+        x2 = csub(a, b);
+        a = x1, b = cmul_conj(x3, tw[(j + q) * st1]);
+        x1 = cadd(a, b);
+        x3 = csub(a, b);
+        sm[b0] = x0, sm[b0 + q] = x1, sm[b0 + 2 * q] = x2, sm[b0 + 3 * q] = x3;
+    }
+}
+
+// Both blocks' stages advance together (one barrier per stage pair).
+__device__ inline void blocks_dif(double2 *s0, double2 *s1, int B, const double2 *tw) {
+    int stages = 0;
+    for (int r = B; r > 1; r >>= 1) ++stages;
+    int s = B;
+    for (; stages >= 2; stages -= 2, s >>= 2) {
+        dif4(s0, B, s, tw);
+        if (s1) dif4(s1, B, s, tw);
+        __syncthreads();
+    }
+    if (stages == 1) {
+        dif2(s0, B, 2, tw);
+        if (s1) dif2(s1, B, 2, tw);
+        __syncthreads();
+    }
+}
+__device__ inline void blocks_dit(double2 *s0, double2 *s1, int B, const double2 *tw) {
+    int stages = 0;
+    for (int r = B; r > 1; r >>= 1) ++stages;
+    int s = 4;
+    if (stages & 1) {
+        dit2(s0, B, 2, tw);
+        if (s1) dit2(s1, B, 2, tw);
+        __syncthreads();
+        s = 8;
+    }
+    for (; s <= B; s <<= 2) {
+        dit4(s0, B, s, tw);
+        if (s1) dit4(s1, B, s, tw);
+        __syncthreads();
+    }
+}
+
+// Pass 2. CTA 0: block 0 (partners inside it, reference pairing
+// src/xcorr.zig:211-229); CTA 1: block 1 (u <-> B-1-u); CTA k >= 2: blocks
+// b and b' = 3*hb - 1 - b for the (k-1)-th pair, hb = 2 * floor_pow2(k-1).
+__global__ void __launch_bounds__(kThreads) middle_blocks(const LagJob *__restrict__ jobs, int B,
+                                                          const double2 *__restrict__ tw) {
+    extern __shared__ double2 sm[];
+    const LagJob job = jobs[blockIdx.y];
+    const int k = blockIdx.x;
+    int64_t b0 = 0, b1 = -1;
+    if (k == 1) {
+        b0 = 1;
+    } else if (k >= 2) {
+        const int64_t i = k - 1;
+        const int64_t p = (int64_t)1 << (63 - __clzll(i));
+        const int64_t hb = 2 * p;
+        b0 = i + p;
+        b1 = 3 * hb - 1 - b0;
+    }
+    double2 *s0 = sm, *s1 = b1 >= 0 ? sm + B : nullptr;
+    double2 *z0 = job.z + b0 * B, *z1 = b1 >= 0 ? job.z + b1 * B : nullptr;
+    for (int u = threadIdx.x; u < B; u += blockDim.x) {
+        s0[u] = z0[u];
+        if (s1) s1[u] = z1[u];
+    }
+    __syncthreads();
+    blocks_dif(s0, s1, B, tw);
+    if (s1) {
+        for (int u = threadIdx.x; u < B; u += blockDim.x) {
+            const double2 za = s0[u], zb = s1[B - 1 - u];
+            s0[u] = cross_term(za, zb);
+            s1[B - 1 - u] = cross_term(zb, za);
+        }
+    } else if (k == 1) {
+        for (int u = threadIdx.x; u < B / 2; u += blockDim.x) {
+            const double2 za = s0[u], zb = s0[B - 1 - u];
+            s0[u] = cross_term(za, zb);
+            s0[B - 1 - u] = cross_term(zb, za);
+        }
+    } else {
+        // block 0: positions 0 and 1 pair with themselves; position a in
+        // [h, 2h) with 3h-1-a.
+        for (int i = threadIdx.x; i < (B > 1 ? B / 2 : 1); i += blockDim.x) {
+            if (i == 0) {
+                s0[0] = cross_term(s0[0], s0[0]);
+                if (B > 1) s0[1] = cross_term(s0[1], s0[1]);
+                continue;
+            }
+            const int p = 1 << (31 - __clz(i));
+            const int h = 2 * p;
+            const int a = i + p, b = 3 * h - 1 - a;
+            const double2 za = s0[a], zb = s0[b];
+            s0[a] = cross_term(za, zb);
+            s0[b] = cross_term(zb, za);
+        }
+    }
+    __syncthreads();
+    blocks_dit(s0, s1, B, tw);
+    for (int u = threadIdx.x; u < B; u += blockDim.x) {
+        z0[u] = s0[u];
+        if (s1) z1[u] = s1[u];
+    }
+}
+
+struct Best {
+    double v;
+    int64_t key;
+};
+__device__ inline Best better(Best a, Best b) {
+    if (b.v > a.v) return b;
+    if (b.v == a.v && b.key < a.key) return b;
+    return a;
+}
+// Position i's key in the CPU's scan order (negative lags first), or -1.
+__device__ inline int64_t lag_key(int64_t i, int64_t n, int64_t max_lag) {
+    if (i >= n - max_lag) return i - (n - max_lag);
+    if (i <= max_lag) return max_lag + i;
+    return -1;
+}
+
+__device__ inline void block_best(Best best, double *pv, int64_t *pk, int64_t slot) {
+    for (int off = 16; off > 0; off >>= 1) {
+        Best o{__shfl_down_sync(0xffffffffu, best.v, off), __shfl_down_sync(0xffffffffu, best.key, off)};
+        best = better(best, o);
+    }
+    __shared__ Best warp_best[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) warp_best[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = better(best, warp_best[w]);
+        pv[slot] = best.v;
+        pk[slot] = best.key;
+    }
+}
+
+// Pass 3: DIT column stages, then this CTA's lag candidates.
+__global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__restrict__ jobs, int G,
+                                                               const double2 *__restrict__ top, double *pv,
+                                                               int64_t *pk, int parts) {
+    extern __shared__ double2 sm[];
+    const LagJob job = jobs[blockIdx.y];
+    const int R = 1 << G, cols = kB >> G > 0 ? (kB >> G) : 1;
+    const int64_t c0 = (int64_t)blockIdx.x * cols;
+    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+        const int t = e / cols, c = e - t * cols;
+        sm[e] = job.z[(int64_t)t * kB + c0 + c];
+    }
+    __syncthreads();
+    column_stages<true>(sm, G, cols, c0, top);
+    const int64_t n = job.n, max_lag = job.biggest - 1;
+    Best best{-INFINITY, INT64_MAX};
+    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+        const int t = e / cols, c = e - t * cols;
+        const int64_t key = lag_key((int64_t)t * kB + c0 + c, n, max_lag);
+        if (key >= 0) best = better(best, Best{fabs(sm[e].x), key});
+    }
+    block_best(best, pv, pk, (int64_t)blockIdx.y * parts + blockIdx.x);
+}
+
+// Single-block transforms (n <= 4096): pack, DIF, cross, DIT, argmax in one CTA.
+template <bool RAW>
+__global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__ jobs, const double2 *__restrict__ tw,
+                                                      double *pv, int64_t *pk) {
+    extern __shared__ double2 sm[];
+    const LagJob job = jobs[blockIdx.y];
+    const int B = (int)job.n;
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    for (int u = threadIdx.x; u < B; u += blockDim.x) sm[u] = packed<RAW>(job, pa, pb, u);
+    __syncthreads();
+    blocks_dif(sm, nullptr, B, tw);
+    for (int i = threadIdx.x; i < (B > 1 ? B / 2 : 1); i += blockDim.x) {
+        if (i == 0) {
+            sm[0] = cross_term(sm[0], sm[0]);
+            if (B > 1) sm[1] = cross_term(sm[1], sm[1]);
+            continue;
+        }
+        const int p = 1 << (31 - __clz(i));
+        const int h = 2 * p;
+        const int a = i + p, b = 3 * h - 1 - a;
+        const double2 za = sm[a], zb = sm[b];
+        sm[a] = cross_term(za, zb);
+        sm[b] = cross_term(zb, za);
+    }
+    __syncthreads();
+    blocks_dit(sm, nullptr, B, tw);
+    const int64_t max_lag = job.biggest - 1;
+    Best best{-INFINITY, INT64_MAX};
+    for (int u = threadIdx.x; u < B; u += blockDim.x) {
+        const int64_t key = lag_key(u, B, max_lag);
+        if (key >= 0) best = better(best, Best{fabs(sm[u].x), key});
+    }
+    block_best(best, pv, pk, blockIdx.y);
+}
+
+__global__ void pick_lag(const LagJob *__restrict__ jobs, int njobs, const double *pv, const int64_t *pk, int parts) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    Best best{-INFINITY, INT64_MAX};
+    for (int p = 0; p < parts; ++p) best = better(best, Best{pv[(int64_t)j * parts + p], pk[(int64_t)j * parts + p]});
+    *jobs[j].lag_out = best.key == INT64_MAX ? 0 : best.key - (jobs[j].biggest - 1);
+}
+
+}  // namespace
+
+void lag_init_attributes() {
+    const int one = kB * (int)sizeof(double2), two = 2 * one;
+    cudaFuncSetAttribute(fwd_columns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(fwd_columns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(inv_columns_argmax, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(small_lag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(small_lag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(middle_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, two);
+}
+
+bool fused_lag_supported(int64_t n) { return n >= 1 && n <= ((int64_t)kB << 12); }
+
+size_t fused_lag_parts(int64_t n) {
+    if (n <= kB) return 1;
+    int G = 0;
+    for (int64_t r = n / kB; r > 1; r >>= 1) ++G;
+    const int cols = (kB >> G) > 0 ? (kB >> G) : 1;
+    return (size_t)(kB / cols);
+}
+
+void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *top,
+                      const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const size_t one = (size_t)kB * sizeof(double2);
+    if (n <= kB) {
+        const size_t smem = (size_t)n * sizeof(double2);
+        if (raw)
+            small_lag<true><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block, pv, pk);
+        else
+            small_lag<false><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block, pv, pk);
+        pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, 1);
+        launch_counter() += 2;
+        return;
+    }
+    int G = 0;
+    for (int64_t r = n / kB; r > 1; r >>= 1) ++G;
+    const int parts = (int)fused_lag_parts(n);
+    const int64_t nblk = n / kB;
+    if (raw)
+        fwd_columns<true><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top);
+    else
+        fwd_columns<false><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top);
+    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kThreads, 2 * one, s>>>(d_jobs, kB, tw_block);
+    inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top, pv, pk, parts);
+    pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
+    launch_counter() += 4;
+}
+
+}  // namespace vqb

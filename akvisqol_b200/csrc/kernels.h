@@ -71,6 +71,13 @@ int argmax_parts(int64_t n);
 void launch_argmax(const double2 *z, const LagJob *d_jobs, int njobs, int64_t n, int64_t stride, double *pv,
                    int64_t *pk, cudaStream_t s);
 
+// k_lag.cu: the fused three-pass lag search (n <= 2^24).
+void lag_init_attributes();
+bool fused_lag_supported(int64_t n);
+size_t fused_lag_parts(int64_t n);  // argmax candidates per job
+void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *top,
+                      const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s);
+
 // k_gammatone.cu
 int gammatone_frames_per_cta(int nb);
 size_t gammatone_tile_size();
