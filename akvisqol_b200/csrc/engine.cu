@@ -165,13 +165,17 @@ Engine::Twiddles Engine::twiddles(size_t n) {
     auto it = twiddles_.find(n);
     if (it != twiddles_.end()) return it->second;
     // top[k] = W_n^k (k < n/2), then the block passes' W_B^k = top[k * n/B].
+    // then the fused lag search's stage-major column twiddles.
     std::vector<double2> t = host::twiddles(n);
     const size_t B = (size_t)fft_block_size((int64_t)n), half = t.size();
     for (size_t k = 0; k < B / 2; ++k) t.push_back(t[k * (n / B)]);
+    const size_t cols_at = t.size();
+    t.resize(cols_at + column_twiddle_count((int64_t)n));
+    fill_column_twiddles(t.data(), (int64_t)n, t.data() + cols_at);
     double2 *d = nullptr;
     VQB_CUDA(cudaMalloc(&d, std::max<size_t>(1, t.size()) * sizeof(double2)));
     if (!t.empty()) VQB_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
-    Twiddles tw{d, d + half};
+    Twiddles tw{d, d + half, d + cols_at};
     twiddles_[n] = tw;
     return tw;
 }
@@ -233,7 +237,7 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
                 const size_t parts = fused_lag_parts(n);
                 double *pv = arena_.alloc_n<double>(parts * cnt);
                 int64_t *pk = arena_.alloc_n<int64_t>(parts * cnt);
-                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.top, tw.block, pv, pk, stream_);
+                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, pv, pk, stream_);
                 continue;
             }
             const int parts = argmax_parts(n);

@@ -112,7 +112,7 @@ public:
     // FFT twiddles of size n on the device: the full table and the block
     // passes' compact one (cached per size).
     struct Twiddles {
-        const double2 *top, *block;
+        const double2 *top, *block, *cols;
     };
     Twiddles twiddles(size_t n);
 

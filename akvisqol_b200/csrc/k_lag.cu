@@ -84,39 +84,117 @@ __device__ inline double2 packed(const LagJob &job, const EnvParams &pa, const E
 
 // G column stages on x[t * cols + c] (t < R = 2^G rows); DIT reverses the
 // stage order. Stage l has span n >> l; the twiddle of the lower point (t, c)
-// is W_{n>>l}^j = top[j << l] with j = (t mod 2h) * 4096 + c0 + c.
+// is W_{n>>l}^j = top[j << l], j = m * 4096 + c0 + c with m = t mod 2h
+// (h = R >> (l+1)). tcol holds those twiddles stage-major,
+// tcol[off(l) + m * 4096 + col] = top[(m * 4096 + col) << l], so a CTA's
+// columns read contiguous runs. Stages go in pairs (radix 4, one barrier)
+// with a radix-2 stage where G is odd.
+__device__ inline int64_t tcol_off(int G, int l) {
+    // sum over l' < l of (R >> (l'+1)) * 4096
+    const int64_t R = (int64_t)1 << G;
+    return (R - (R >> l)) * kB;
+}
+
 template <bool DIT>
-__device__ inline void column_stages(double2 *x, int G, int cols, int64_t c0, const double2 *__restrict__ top) {
-    const int R = 1 << G;
-    const int pairs = (R >> 1) * cols;
-    for (int li = 0; li < G; ++li) {
-        const int l = DIT ? G - 1 - li : li;
-        const int h = R >> (l + 1);
-        for (int bf = threadIdx.x; bf < pairs; bf += blockDim.x) {
-            const int pr = bf / cols, c = bf - pr * cols;
-            const int t = (pr / h) * 2 * h + (pr % h);
-            const int64_t j = (int64_t)(t % (2 * h)) * kB + c0 + c;
-            const double2 w = top[j << l];
-            double2 *pa = x + t * cols + c, *pb = x + (t + h) * cols + c;
-            const double2 a = *pa;
-            if (!DIT) {
-                const double2 b = *pb;
-                *pa = cadd(a, b);
-                *pb = cmul(csub(a, b), w);
-            } else {
-                const double2 b = cmul_conj(*pb, w);
-                *pa = cadd(a, b);
-                *pb = csub(a, b);
-            }
+__device__ inline void column_stage2(double2 *x, int G, int l, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+    const int R = 1 << G, h = R >> (l + 1);
+    const double2 *tw = tcol + tcol_off(G, l) + c0;
+    for (int bf = threadIdx.x; bf < (R >> 1) * cols; bf += blockDim.x) {
+        const int pr = bf / cols, c = bf - pr * cols;
+        const int m = pr % h;
+        const int t = (pr / h) * 2 * h + m;
+        const double2 w = tw[(int64_t)m * kB + c];
+        double2 *pa = x + t * cols + c, *pb = x + (t + h) * cols + c;
+        const double2 a = *pa;
+        if (!DIT) {
+            const double2 b = *pb;
+            *pa = cadd(a, b);
+            *pb = cmul(csub(a, b), w);
+        } else {
+            const double2 b = cmul_conj(*pb, w);
+            *pa = cadd(a, b);
+            *pb = csub(a, b);
         }
-        __syncthreads();
+    }
+}
+
+// Stages l (span S) and l+1 (span S/2) on 4-row groups t0 + {0,q,2q,3q},
+// q = R >> (l+2): stage l pairs (0,2),(1,3) with twiddle rows m and m+q,
+// stage l+1 pairs (0,1),(2,3) with row m. DIT runs stage l+1 first.
+template <bool DIT>
+__device__ inline void column_stage4(double2 *x, int G, int l, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+    const int R = 1 << G, q = R >> (l + 2);
+    const double2 *tw1 = tcol + tcol_off(G, l) + c0, *tw2 = tcol + tcol_off(G, l + 1) + c0;
+    for (int g = threadIdx.x; g < (R >> 2) * cols; g += blockDim.x) {
+        const int pr = g / cols, c = g - pr * cols;
+        const int m = pr % q;
+        const int t0 = (pr / q) * 4 * q + m;
+        double2 *p0 = x + t0 * cols + c, *p1 = p0 + q * cols, *p2 = p1 + q * cols, *p3 = p2 + q * cols;
+        double2 x0 = *p0, x1 = *p1, x2 = *p2, x3 = *p3;
+        const double2 wa = tw1[(int64_t)m * kB + c], wb = tw1[(int64_t)(m + q) * kB + c];
+        const double2 w2 = tw2[(int64_t)m * kB + c];
+        double2 a, b;
+        if (!DIT) {
+            a = x0, b = x2;
+            x0 = cadd(a, b);
+            x2 = cmul(csub(a, b), wa);
+            a = x1, b = x3;
+            x1 = cadd(a, b);
+            x3 = cmul(csub(a, b), wb);
+            a = x0, b = x1;
+            x0 = cadd(a, b);
+            x1 = cmul(csub(a, b), w2);
+            a = x2, b = x3;
+            x2 = cadd(a, b);
+            x3 = cmul(csub(a, b), w2);
+        } else {
+            a = x0, b = cmul_conj(x1, w2);
+            x0 = cadd(a, b);
+            x1 = csub(a, b);
+            a = x2, b = cmul_conj(x3, w2);
+            x2 = cadd(a, b);
+            x3 = csub(a, b);
+            a = x0, b = cmul_conj(x2, wa);
+            x0 = cadd(a, b);
+            x2 = csub(a, b);
+            a = x1, b = cmul_conj(x3, wb);
+            x1 = cadd(a, b);
+            x3 = csub(a, b);
+        }
+        *p0 = x0, *p1 = x1, *p2 = x2, *p3 = x3;
+    }
+}
+
+template <bool DIT>
+__device__ inline void column_stages(double2 *x, int G, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+    if (!DIT) {
+        int l = 0;
+        for (; l + 1 < G; l += 2) {
+            column_stage4<false>(x, G, l, cols, c0, tcol);
+            __syncthreads();
+        }
+        if (l < G) {
+            column_stage2<false>(x, G, l, cols, c0, tcol);
+            __syncthreads();
+        }
+    } else {
+        int l = G - 1;
+        if (G & 1) {
+            column_stage2<true>(x, G, l, cols, c0, tcol);
+            __syncthreads();
+            --l;
+        }
+        for (; l >= 1; l -= 2) {
+            column_stage4<true>(x, G, l - 1, cols, c0, tcol);
+            __syncthreads();
+        }
     }
 }
 
 // Pass 1: pack + DIF column stages. grid (n / (R*cols) ... = 4096/cols, jobs).
 template <bool RAW>
 __global__ void __launch_bounds__(kThreads) fwd_columns(const LagJob *__restrict__ jobs, int G,
-                                                        const double2 *__restrict__ top) {
+                                                        const double2 *__restrict__ tcol) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
     const int R = 1 << G, cols = kB >> G > 0 ? (kB >> G) : 1;
@@ -131,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) fwd_columns(const LagJob *__restrict
         sm[e] = packed<RAW>(job, pa, pb, (int64_t)t * kB + c0 + c);
     }
     __syncthreads();
-    column_stages<false>(sm, G, cols, c0, top);
+    column_stages<false>(sm, G, cols, c0, tcol);
     for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
         const int t = e / cols, c = e - t * cols;
         job.z[(int64_t)t * kB + c0 + c] = sm[e];
@@ -242,7 +320,7 @@ __device__ inline void blocks_dit(double2 *s0, double2 *s1, int B, const double2
 // Pass 2. CTA 0: block 0 (partners inside it, reference pairing
 // src/xcorr.zig:211-229); CTA 1: block 1 (u <-> B-1-u); CTA k >= 2: blocks
 // b and b' = 3*hb - 1 - b for the (k-1)-th pair, hb = 2 * floor_pow2(k-1).
-__global__ void __launch_bounds__(kThreads) middle_blocks(const LagJob *__restrict__ jobs, int B,
+__global__ void __launch_bounds__(2 * kThreads) middle_blocks(const LagJob *__restrict__ jobs, int B,
                                                           const double2 *__restrict__ tw) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
@@ -335,7 +413,7 @@ __device__ inline void block_best(Best best, double *pv, int64_t *pk, int64_t sl
 
 // Pass 3: DIT column stages, then this CTA's lag candidates.
 __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__restrict__ jobs, int G,
-                                                               const double2 *__restrict__ top, double *pv,
+                                                               const double2 *__restrict__ tcol, double *pv,
                                                                int64_t *pk, int parts) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
@@ -346,7 +424,7 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
         sm[e] = job.z[(int64_t)t * kB + c0 + c];
     }
     __syncthreads();
-    column_stages<true>(sm, G, cols, c0, top);
+    column_stages<true>(sm, G, cols, c0, tcol);
     const int64_t n = job.n, max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
     for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
@@ -426,7 +504,20 @@ size_t fused_lag_parts(int64_t n) {
     return (size_t)(kB / cols);
 }
 
-void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *top,
+size_t column_twiddle_count(int64_t n) { return n <= kB ? 0 : (size_t)(n - kB); }
+
+void fill_column_twiddles(const double2 *top, int64_t n, double2 *out) {
+    if (n <= kB) return;
+    int G = 0;
+    for (int64_t r = n / kB; r > 1; r >>= 1) ++G;
+    const int64_t R = (int64_t)1 << G;
+    size_t k = 0;
+    for (int l = 0; l < G; ++l)
+        for (int64_t m = 0; m < (R >> (l + 1)); ++m)
+            for (int64_t col = 0; col < kB; ++col) out[k++] = top[(m * kB + col) << l];
+}
+
+void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
                       const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s) {
     if (njobs <= 0) return;
     const size_t one = (size_t)kB * sizeof(double2);
@@ -445,11 +536,12 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
     const int parts = (int)fused_lag_parts(n);
     const int64_t nblk = n / kB;
     if (raw)
-        fwd_columns<true><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top);
+        fwd_columns<true><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
     else
-        fwd_columns<false><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top);
-    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kThreads, 2 * one, s>>>(d_jobs, kB, tw_block);
-    inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, top, pv, pk, parts);
+        fwd_columns<false><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
+    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), 2 * kThreads, 2 * one, s>>>(d_jobs, kB,
+                                                                                                tw_block);
+    inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);
     pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
     launch_counter() += 4;
 }

@@ -75,7 +75,11 @@ void launch_argmax(const double2 *z, const LagJob *d_jobs, int njobs, int64_t n,
 void lag_init_attributes();
 bool fused_lag_supported(int64_t n);
 size_t fused_lag_parts(int64_t n);  // argmax candidates per job
-void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *top,
+// Stage-major column twiddles of the global stages (host-side, from the
+// full table top[k] = W_n^k): column_twiddle_count(n) entries.
+size_t column_twiddle_count(int64_t n);
+void fill_column_twiddles(const double2 *top, int64_t n, double2 *out);
+void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
                       const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s);
 
 // k_gammatone.cu
