@@ -133,6 +133,7 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_log10": (c_int, [D, c_size_t, D]),
         "visqol_b200_nsim_table": (c_int, [D, c_size_t, D, c_size_t, c_size_t, c_size_t, c_size_t, I64, I64, I64, D]),
         "visqol_b200_dp": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
+        "visqol_b200_dp_static": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
         "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
         "visqol_b200_peak": (c_int, [c_int, D]),
     }
@@ -159,6 +160,7 @@ EXPORTS = [
     "visqol_b200_measure_batch", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
     "visqol_b200_spectrogram", "visqol_b200_envelope_lag", "visqol_b200_best_lag", "visqol_b200_fft",
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
+    "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
 ]
 
@@ -430,7 +432,10 @@ def nsim_table(ref_spec, deg_spec, patch: int, ref_idx, lo, hi) -> np.ndarray:
     return out[: ri.size * nfd].reshape(ri.size, nfd)
 
 
-def dp(sims, lo, hi):
+def dp(sims, lo, hi, static_scratch=False):
+    """Matched offset, validity and reached count per patch; with
+    static_scratch the call goes through visqol_b200_dp_static, which takes
+    its device buffers from the library's reserved array."""
     s = np.ascontiguousarray(sims, dtype=np.float64)
     np_, nfd = s.shape
     lo = np.ascontiguousarray(lo, dtype=np.int64)
@@ -438,8 +443,9 @@ def dp(sims, lo, hi):
     off = np.zeros(np_, np.int64)
     valid = np.zeros(np_, np.uint8)
     reached = c_size_t()
-    _check(lib.visqol_b200_dp(_ptr(s), np_, nfd, _i64(lo), _i64(hi), _i64(off),
-                              valid.ctypes.data_as(POINTER(c_uint8)), ctypes.byref(reached)))
+    fn = lib.visqol_b200_dp_static if static_scratch else lib.visqol_b200_dp
+    _check(fn(_ptr(s), np_, nfd, _i64(lo), _i64(hi), _i64(off), valid.ctypes.data_as(POINTER(c_uint8)),
+              ctypes.byref(reached)))
     return off, valid, reached.value
 
 

@@ -129,6 +129,20 @@ int visqol_b200_dp(const double *sims, size_t np, size_t nf_deg,
                    const int64_t *lo, const int64_t *hi,
                    int64_t *offset, uint8_t *valid, size_t *reached);
 
+/* visqol_b200_dp without device allocation. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory at
+ * call time (a process whose caching allocator already holds the free HBM,
+ * or one that cannot let cudaFree wait for the whole device). Its device
+ * buffers come from one ~6 MiB array reserved in the library image.
+ * Limits: np <= 2048 and np * nf_deg <= 262144, else
+ * VISQOL_E_INVALID_ARGUMENT. The first call on a device resolves the array
+ * (make it before any stream capture); calls that overlap in time on one
+ * device share the array and race, so serialise them. Same arguments and
+ * results as visqol_b200_dp. */
+int visqol_b200_dp_static(const double *sims, size_t np, size_t nf_deg,
+                          const int64_t *lo, const int64_t *hi,
+                          int64_t *offset, uint8_t *valid, size_t *reached);
+
 /* Per-band NSIM statistics of one patch pair (reference
  * src/nsim.zig:427-510); *mean gets the mean of the band means. */
 int visqol_b200_patch_similarity(const double *ref, const double *deg,
