@@ -274,9 +274,13 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
         return fail(VISQOL_E_INVALID_ARGUMENT, "invalid precision " + std::to_string(o.precision));
     if (o.backend != VISQOL_BACKEND_CUDA)
         return fail(VISQOL_E_BACKEND, "BackendUnavailable: this libvisqol serves backend cuda (2) only");
-    if (o.precision == VISQOL_PRECISION_FAST || o.precision == VISQOL_PRECISION_BALANCED)
-        return fail(VISQOL_E_BACKEND, "BackendUnavailable: only the exact (f64) form is built");
     auto c = std::make_unique<visqol_ctx>();
+    // EXACT (and AUTO, which resolves to exact on a device with native f64)
+    // reproduce the CPU path; FAST runs the gammatone's later stages in f32;
+    // BALANCED keeps f64 throughout but with FMA and reassociated sums.
+    c->opt.form = o.precision == VISQOL_PRECISION_FAST       ? vqb::kFormF32
+                  : o.precision == VISQOL_PRECISION_BALANCED ? vqb::kFormF64
+                                                             : vqb::kFormExact;
     c->opt.speech = o.mode == VISQOL_MODE_SPEECH;
     c->opt.radius = o.search_window_radius > 0 ? o.search_window_radius : 60;
     c->opt.unscaled_speech = o.use_unscaled_speech_mos_mapping != 0;

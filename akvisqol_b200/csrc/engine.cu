@@ -138,6 +138,7 @@ Engine::~Engine() {
     if (side_) cudaStreamDestroy(side_);
     for (auto &kv : rates_) {
         cudaFree(kv.second.d_coeffs);
+        cudaFree(kv.second.d_fast_coeffs);
         cudaFree(kv.second.d_hann);
     }
     for (auto &kv : twiddles_) cudaFree(const_cast<double2 *>(kv.second.top));
@@ -157,6 +158,10 @@ const Engine::RateCache &Engine::rate_cache(uint32_t sr) {
     VQB_CUDA(cudaMalloc(&rc.d_coeffs, nb_ * sizeof(BandCoeffs)));
     VQB_CUDA(cudaMalloc(&rc.d_hann, std::max<size_t>(1, w.size()) * sizeof(double)));
     VQB_CUDA(cudaMemcpy(rc.d_coeffs, rc.fb.run.data(), nb_ * sizeof(BandCoeffs), cudaMemcpyHostToDevice));
+    std::vector<FastBandCoeffs> fast(nb_);
+    fill_fast_band_coeffs(rc.fb.run.data(), rc.fb.cf.data(), (int)nb_, fast.data());
+    VQB_CUDA(cudaMalloc(&rc.d_fast_coeffs, nb_ * sizeof(FastBandCoeffs)));
+    VQB_CUDA(cudaMemcpy(rc.d_fast_coeffs, fast.data(), nb_ * sizeof(FastBandCoeffs), cudaMemcpyHostToDevice));
     if (!w.empty()) VQB_CUDA(cudaMemcpy(rc.d_hann, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
     return rates_.emplace(sr, std::move(rc)).first->second;
 }
@@ -250,6 +255,15 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
             launch_argmax(z, d_jobs, (int)cnt, n, n, pv, pk, stream_);
         }
     }
+}
+
+void Engine::launch_sums(const std::vector<SumJob> &sums) {
+    if (sums.empty()) return;
+    const SumJob *d = upload(sums);
+    if (opt_.form != kFormExact)
+        launch_envelope_stats_tree(d, (int)sums.size(), arena_.alloc_n<double>(sums.size() * kTreeParts * 3), stream_);
+    else
+        launch_envelope_stats(d, (int)sums.size(), stream_);
 }
 
 void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags) {
@@ -402,7 +416,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     auto run_gammatone = [&](const std::vector<SpecJob> &jobs, cudaStream_t st) {
         if (jobs.empty()) return;
         SpecJob *d_jobs = upload(jobs);
-        const int F = gammatone_frames_per_cta(nbi);
+        const int F = opt_.form == kFormF32 ? gammatone_fast_frames_per_cta() : gammatone_frames_per_cta(nbi);
         const size_t tsz = gammatone_tile_size();
         std::vector<char> tiles;
         int ntiles = 0;
@@ -422,7 +436,12 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         }
         const size_t slot = 2 * timing_.gammatone_launches;
         VQB_CUDA(cudaEventRecord(gt_events_[slot], st));
-        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
+        if (opt_.form == kFormF32)
+            launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
+        else if (opt_.form == kFormF64)
+            launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
+        else
+            launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
         VQB_CUDA(cudaEventRecord(gt_events_[slot + 1], st));
         timing_.gammatone_launches += 1;
         timing_.gammatone_rms += rms;
@@ -470,7 +489,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                 s.trace.fft_nlogn += 2.0 * (double)j.n * std::log2((double)j.n);
             }
         }
-        if (!sums.empty()) launch_envelope_stats(upload(sums), (int)sums.size(), stream_);
+        launch_sums(sums);
         launch_lag_jobs(lag_jobs, false);
         std::vector<char> args;
         const size_t asz = aligned_energy_args_size();
@@ -483,7 +502,11 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                                      (int64_t)s.rl, d_lags + i, s.stats + 8);
             ++na;
         }
-        if (na) launch_aligned_energy(upload_bytes(args.data(), args.size()), na, stream_);
+        if (na && opt_.form != kFormExact)
+            launch_aligned_energy_tree(upload_bytes(args.data(), args.size()), na,
+                                       arena_.alloc_n<double>((size_t)na * kTreeParts * 3), stream_);
+        else if (na)
+            launch_aligned_energy(upload_bytes(args.data(), args.size()), na, stream_);
     }
     int64_t *h_lags = pinned_.alloc_n<int64_t>(n);
     double *h_stats = pinned_.alloc_n<double>(10 * n);
@@ -701,7 +724,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
             }
         }
         // ---- 5: slice lags --------------------------------------------------
-        launch_envelope_stats(upload(slice_sums), (int)slice_sums.size(), stream_);
+        launch_sums(slice_sums);
         launch_lag_jobs(slice_lags, false);
         int64_t *h_sl = pinned_.alloc_n<int64_t>(n_slices);
         d2h(h_sl, d_slice_lags, n_slices * sizeof(int64_t));

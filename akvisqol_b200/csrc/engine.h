@@ -12,6 +12,7 @@
 
 #include "device.cuh"
 #include "host_model.h"
+#include "kernels.h"
 
 namespace vqb {
 
@@ -21,6 +22,8 @@ struct Options {
     bool unscaled_speech = false;
     bool disable_global_alignment = false;
     bool disable_realignment = false;
+    // Arithmetic form (kFormExact, kFormF32, kFormF64).
+    int32_t form = kFormExact;
 };
 
 struct PairTrace {
@@ -121,8 +124,11 @@ private:
         host::Filterbank fb;
         host::Geometry geo;
         BandCoeffs *d_coeffs = nullptr;
+        FastBandCoeffs *d_fast_coeffs = nullptr;
         double *d_hann = nullptr;
     };
+    // Envelope statistics of sum jobs: serial (exact) or tree (fast).
+    void launch_sums(const std::vector<SumJob> &sums);
     const RateCache &rate_cache(uint32_t sample_rate);
 
     // Envelope (or raw) lag search for jobs whose a/b/stat pointers are set;

@@ -158,6 +158,130 @@ __global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const
     }
 }
 
+// ---- fast form: tree reductions -------------------------------------------
+// The fast form does not reproduce the CPU's rounding, so its statistics are
+// deterministic tree sums: kTreeParts CTAs per signal each reduce a
+// contiguous range (strided, coalesced loads; warp shuffles; shared memory)
+// into scratch, and one warp per signal adds the parts in order.
+constexpr int kTreeThreads = 256;
+
+__device__ inline double block_sum(double v, double *sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    return t;  // valid in thread 0
+}
+
+__device__ inline void part_range(int64_t n, int64_t &lo, int64_t &hi) {
+    const int64_t per = (n + kTreeParts - 1) / kTreeParts;
+    lo = per * blockIdx.x;
+    hi = lo + per < n ? lo + per : n;
+}
+
+// Partial sums of x, (-1)^k x and x^2 over this CTA's range.
+__global__ void __launch_bounds__(kTreeThreads) stats_tree_parts(const SumJob *__restrict__ jobs,
+                                                                 double *__restrict__ scratch) {
+    __shared__ double sm[kTreeThreads / 32];
+    const SumJob job = jobs[blockIdx.y];
+    int64_t lo, hi;
+    part_range(job.sig.len, lo, hi);
+    double s = 0.0, a = 0.0, e = 0.0;
+#pragma unroll 4
+    for (int64_t k = lo + threadIdx.x; k < hi; k += kTreeThreads) {
+        const double x = vsig_at(job.sig, k);
+        s += x;
+        a += (k & 1) ? -x : x;
+        e = __fma_rn(x, x, e);
+    }
+    s = block_sum(s, sm);
+    a = block_sum(a, sm);
+    e = block_sum(e, sm);
+    if (threadIdx.x == 0) {
+        double *p = scratch + ((int64_t)blockIdx.y * kTreeParts + blockIdx.x) * 3;
+        p[0] = s;
+        p[1] = a;
+        p[2] = e;
+    }
+}
+
+// out[0] = sum x, out[1] = sum (-1)^k (x - mean) = alt - mean * (len odd),
+// out[2] = sum x^2.
+__global__ void __launch_bounds__(32) stats_tree_finish(const SumJob *__restrict__ jobs,
+                                                        const double *__restrict__ scratch) {
+    const SumJob job = jobs[blockIdx.x];
+    const double *p = scratch + (int64_t)blockIdx.x * kTreeParts * 3;
+    const int lane = threadIdx.x;
+    double s = p[lane * 3], a = p[lane * 3 + 1], e = p[lane * 3 + 2];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        e += __shfl_down_sync(0xffffffffu, e, o);
+    }
+    if (lane == 0) {
+        const int64_t len = job.sig.len;
+        const double mean = len > 0 ? s / (double)len : 0.0;
+        job.out[0] = s;
+        job.out[1] = (len & 1) ? a - mean : a;
+        job.out[2] = e;
+    }
+}
+
+// Aligned energy (as aligned_energy_kernel) as a tree sum.
+__device__ inline void aligned_range(const AlignedEnergyArgs &job, int64_t &skip, int64_t &alen) {
+    const int64_t lag = *job.lag;
+    const int64_t half_ref = job.ref_len / 2;
+    const int64_t mag = lag < 0 ? -lag : lag;
+    const int64_t L = job.deg.len;
+    skip = 0;
+    alen = L;
+    if (lag != 0 && mag <= half_ref) {
+        if (lag < 0) {
+            skip = -lag < L ? -lag : L;
+            alen = L - skip;
+        } else {
+            alen = L + lag;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTreeThreads) aligned_tree_parts(const AlignedEnergyArgs *__restrict__ jobs,
+                                                                   double *__restrict__ scratch) {
+    __shared__ double sm[kTreeThreads / 32];
+    const AlignedEnergyArgs job = jobs[blockIdx.y];
+    int64_t skip, alen;
+    aligned_range(job, skip, alen);
+    int64_t lo, hi;
+    part_range(job.deg.len - skip, lo, hi);
+    double e = 0.0;
+#pragma unroll 4
+    for (int64_t k = lo + threadIdx.x; k < hi; k += kTreeThreads) {
+        const double x = vsig_at(job.deg, skip + k);
+        e = __fma_rn(x, x, e);
+    }
+    e = block_sum(e, sm);
+    if (threadIdx.x == 0) scratch[((int64_t)blockIdx.y * kTreeParts + blockIdx.x) * 3] = e;
+}
+
+__global__ void __launch_bounds__(32) aligned_tree_finish(const AlignedEnergyArgs *__restrict__ jobs,
+                                                          const double *__restrict__ scratch) {
+    const AlignedEnergyArgs job = jobs[blockIdx.x];
+    double e = scratch[((int64_t)blockIdx.x * kTreeParts + threadIdx.x) * 3];
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+    if (threadIdx.x == 0) {
+        int64_t skip, alen;
+        aligned_range(job, skip, alen);
+        job.out[0] = e;
+        job.out[1] = (double)alen;
+    }
+}
+
 __host__ __device__ inline int64_t next_pow_two(int64_t x) {
     int64_t n = 1;
     while (n < x) n <<= 1;
@@ -256,6 +380,22 @@ void launch_aligned_energy(const void *d_args, int njobs, cudaStream_t s) {
     aligned_energy_kernel<<<(njobs + per_block - 1) / per_block, 32 * per_block, 0, s>>>(
         static_cast<const AlignedEnergyArgs *>(d_args), njobs);
     launch_counter() += 1;
+}
+
+void launch_envelope_stats_tree(const SumJob *d_jobs, int njobs, double *d_scratch, cudaStream_t s) {
+    if (njobs <= 0) return;
+    static_assert(kTreeParts == 32, "the finishing warp adds one part per lane");
+    stats_tree_parts<<<dim3(kTreeParts, (unsigned)njobs), kTreeThreads, 0, s>>>(d_jobs, d_scratch);
+    stats_tree_finish<<<njobs, 32, 0, s>>>(d_jobs, d_scratch);
+    launch_counter() += 2;
+}
+
+void launch_aligned_energy_tree(const void *d_args, int njobs, double *d_scratch, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const auto *a = static_cast<const AlignedEnergyArgs *>(d_args);
+    aligned_tree_parts<<<dim3(kTreeParts, (unsigned)njobs), kTreeThreads, 0, s>>>(a, d_scratch);
+    aligned_tree_finish<<<njobs, 32, 0, s>>>(a, d_scratch);
+    launch_counter() += 2;
 }
 
 size_t aligned_energy_args_size() { return sizeof(AlignedEnergyArgs); }

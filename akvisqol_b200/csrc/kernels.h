@@ -45,6 +45,26 @@ struct DpJob {
     uint8_t *valid;   // np
 };
 
+// Per-band coefficients of the fast gammatone forms (k_gammatone_fast.cu).
+struct FastBandCoeffs {
+    // f32 form: stage 1 in f64, stages 2-4 in f32
+    double n0, n1, d1, d2;     // stage 1: gain-folded numerator and poles
+    double post;               // |a0^3|, the numerator gain of stages 2-4
+    float beta[3];             // stages 2-4 numerators 1 + beta z^-1
+    float p1h, p1l, p2h, p2l;  // poles d1, d2 as hi + lo f32 pairs
+    int32_t direct_i;          // 1: direct form I, 0: transposed direct form II
+    // f64 FMA form: all four stages direct form I with unit-leading numerators
+    double beta64[4];          // numerators 1 + beta64 z^-1
+    double post64;             // |a0^4 / gain|
+};
+
+// Arithmetic forms of the batch pipeline.
+enum Form : int32_t {
+    kFormExact = 0,  // f64, no FMA, the CPU's operation order (bit-identical stages)
+    kFormF32 = 1,    // gammatone stages 2-4 in f32 (stage 1 f64), tree-summed statistics
+    kFormF64 = 2,    // gammatone in f64 with FMA (direct form I), tree-summed statistics
+};
+
 // Kernels launched by this thread so far (each launcher counts its own).
 uint64_t &launch_counter();
 
@@ -58,6 +78,12 @@ void launch_pack(const LagJob *d_jobs, int njobs, int64_t max_n, bool raw, cudaS
 size_t scale_args_size();
 void fill_scale_args(void *dst, const VSig &src, double factor, double *out);
 void launch_scale(const void *d_args, int njobs, int64_t max_len, cudaStream_t s);
+
+// Fast form: the same statistics as deterministic tree reductions.
+// scratch: kTreeParts * 3 doubles per job.
+constexpr int kTreeParts = 32;
+void launch_envelope_stats_tree(const SumJob *d_jobs, int njobs, double *d_scratch, cudaStream_t s);
+void launch_aligned_energy_tree(const void *d_args, int njobs, double *d_scratch, cudaStream_t s);
 
 // k_fft.cu
 void fft_init_attributes();
@@ -89,6 +115,15 @@ void fill_gammatone_tile(void *dst, int job, int frame0);
 void launch_gammatone(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const BandCoeffs *d_coeffs, int nb,
                       const double *d_hann, int window, int hop, cudaStream_t s);
 void launch_copy_frames(const CopyJob *d_jobs, int njobs, int nb, int max_cols, cudaStream_t s);
+
+// k_gammatone_fast.cu (tiles as fill_gammatone_tile writes them)
+int gammatone_fast_frames_per_cta();
+void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, FastBandCoeffs *out);
+void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
+                           int nb, const double *d_hann, int window, int hop, cudaStream_t s);
+// f64 FMA form: tiles of gammatone_frames_per_cta(nb) frames, as the exact kernel.
+void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
+                             int nb, const double *d_hann, int window, int hop, cudaStream_t s);
 
 // k_spec.cu
 void launch_prep(const PrepJob *d_jobs, int njobs, int nb, cudaStream_t s);

@@ -9,7 +9,12 @@ copy); ``e2e`` times the public call with pinned host buffers, host-to-device
 copies and result read-back included. Each step's inputs (~0.5 GB) exceed
 the 126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+The headline form is --precision (fast: f32 gammatone stages; balanced:
+f64 with FMA; exact: the CPU path's f64 operation order); the other forms
+are timed the same way and reported under "forms", each with its largest
+|dMOS| against the CPU model on the baseline sample.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--precision F]
   python bench.py --impl reference ...   # the reference CPU model (oracle), all host threads
 
 With torchrun (N > 1) every rank scores its own batch (weak scaling, no
@@ -32,7 +37,16 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), exact FP64 form, 1 B200"
+METRICS = {
+    "fast": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), FP32 form, 1 B200",
+    "balanced": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), FP64 FMA form, 1 B200",
+    "exact": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), exact FP64 form, 1 B200",
+}
+DTYPES = {"fast": "f32 (gammatone stages 2-4; stage 1, lags, NSIM, DP in f64)", "balanced": "f64 (FMA)",
+          "exact": "f64"}
+# gammatone: pipe-peak kind of visqol_b200_peak and flops counted per sample
+ROOF = {"exact": (0, 31.0, "fp64-pipe (mul/add)"), "balanced": (1, 27.0, "fp64-pipe (fma)"),
+        "fast": (2, 32.0, "fp32-pipe (fma), stage 1 on the fp64 pipe")}
 WORKLOAD = "audio-mode pairs, 10 s at 48 kHz (480,000 samples; degraded 481,776), seeded synthetic music-like generator"
 
 
@@ -44,6 +58,8 @@ def parse():
     p.add_argument("--batch", type=int, default=64)
     p.add_argument("--seconds", type=float, default=10.0)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fast", choices=["fast", "balanced", "exact"])
+    p.add_argument("--only", action="store_true", help="time the --precision form alone")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -165,7 +181,7 @@ def run_reference(args, rank, world):
     ms = 1e3 * float(np.mean(times))
     value = len(pairs) / (ms / 1e3)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+        "impl": "reference", "metric": METRICS[args.precision], "value": value, "unit": "pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "batch_per_step": len(pairs), "note": "inputs exceed L2"},
@@ -183,7 +199,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     B = args.batch
     pairs = make_pairs(B, args.seconds, 0x5EED_0000 + 1000003 * rank)
-    ctx = native.Context(mode=native.MODE_AUDIO, precision="exact")
+    forms = [args.precision] + ([] if args.only else [f for f in ("fast", "balanced", "exact") if f != args.precision])
+    ctxs = {f: native.Context(mode=native.MODE_AUDIO, precision=f) for f in set(forms) | {"exact"}}
     # device-resident inputs (torch is only the allocator here)
     d_ref = [torch.from_numpy(r).cuda() for r, _ in pairs]
     d_deg = [torch.from_numpy(d).cuda() for _, d in pairs]
@@ -193,34 +210,56 @@ def run_ours(args, rank, world, local):
     len_d = [t.numel() for t in d_deg]
     torch.cuda.synchronize()
 
-    def dev_step():
-        out = ctx.measure_batch_traced(ptr_r, ptr_d, 48000, device_inputs=True, ref_lens=len_r, deg_lens=len_d)
-        return out, ctx.last_timing()
+    def timed(form, clocks_box=None):
+        ctx = ctxs[form]
 
-    for _ in range(args.warmup):
-        dev_step()
-    torch.cuda.synchronize()
-    barrier(world)
-    timings, walls, results = [], [], None
-    with Clocks(local) as clocks:
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            results, t = dev_step()
-            walls.append(time.perf_counter() - t0)
-            timings.append(t)
-    torch.cuda.synchronize()
-    barrier(world)
-    dev_ms = sum(t["total_ms"] for t in timings)
-    dev_ms_max = all_max(dev_ms, world)
-    ms_per_step = dev_ms_max / args.steps
-    value = world * B * args.steps / (dev_ms_max / 1e3)
-    failures = sum(1 for c, _, _ in results if c != 0)
+        def dev_step():
+            out = ctx.measure_batch_traced(ptr_r, ptr_d, 48000, device_inputs=True, ref_lens=len_r, deg_lens=len_d)
+            return out, ctx.last_timing()
+
+        for _ in range(args.warmup):
+            dev_step()
+        torch.cuda.synchronize()
+        barrier(world)
+        timings, walls, results = [], [], None
+        with Clocks(local) as clocks:
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                results, t = dev_step()
+                walls.append(time.perf_counter() - t0)
+                timings.append(t)
+        torch.cuda.synchronize()
+        barrier(world)
+        dev_ms_max = all_max(sum(t["total_ms"] for t in timings), world)
+        kind, flops_per_sample, bound = ROOF[form]
+        gt_ms = sum(t["gammatone_kernel_ms"] for t in timings)
+        gt_launches = sum(t["gammatone_launches"] for t in timings)
+        gt_rms = sum(t["gammatone_rms"] for t in timings)
+        window = timings[0]["gammatone_window"]
+        achieved = flops_per_sample * window * gt_rms / (gt_ms / 1e3) / 1e12 if gt_ms > 0 else None
+        peak = native.peak_tflops(kind)
+        return {
+            "value": world * B * args.steps / (dev_ms_max / 1e3), "ms_per_step": dev_ms_max / args.steps,
+            "walls": walls, "timings": timings, "results": results, "clocks": clocks.summary(),
+            "failures": sum(1 for c, _, _ in results if c != 0),
+            "gt_rms": gt_rms, "gt_launches": gt_launches,
+            "roofline": {"bound": bound, "kernel": "gammatone", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved and peak else None,
+                         "flops_per_rms": flops_per_sample * window,
+                         "peak_source": f"measured here: visqol_b200_peak kind {kind}"},
+        }
+
+    runs = {f: timed(f) for f in forms}
+    head = runs[args.precision]
+    ctx = ctxs[args.precision]
 
     # e2e: public API, pinned host buffers, copies inside the timed region
     pin_r = [torch.from_numpy(r).pin_memory().numpy() for r, _ in pairs]
     pin_d = [torch.from_numpy(d).pin_memory().numpy() for _, d in pairs]
     for _ in range(args.warmup):
-        ctx.measure_batch(pin_r, pin_d, 48000)
+        for o in ctx.measure_batch(pin_r, pin_d, 48000):
+            if not isinstance(o, native.NativeError):
+                native.free(o)
     barrier(world)
     e2e_times, h2d, d2h = [], 0, 0
     for _ in range(args.steps):
@@ -237,20 +276,14 @@ def run_ours(args, rank, world, local):
     e2e_value = world * B * args.steps / e2e_s
     signal_bytes = sum(r.nbytes + d.nbytes for r, d in pairs)
 
-    # roofline of the dominant kernel (gammatone, f64 pipe, no FMA)
-    gt_ms = sum(t["gammatone_kernel_ms"] for t in timings)
-    gt_launches = sum(t["gammatone_launches"] for t in timings)
-    gt_rms = sum(t["gammatone_rms"] for t in timings)
-    window = timings[0]["gammatone_window"]
-    flops = 31.0 * window * gt_rms
-    achieved = flops / (gt_ms / 1e3) / 1e12 if gt_ms > 0 else None
-    peak = native.peak_tflops(0)
-    traffic = None
+    roof = dict(head["roofline"])
+    roof["traffic"] = None
     prof = ROOT / "profiles" / "gammatone_traffic.json"
     if prof.is_file():
         per_rms = json.loads(prof.read_text()).get("dram_bytes_per_rms_audio48k")
         if per_rms:
-            traffic = per_rms * gt_rms / max(1, gt_launches)
+            roof["traffic"] = per_rms * head["gt_rms"] / max(1, head["gt_launches"])
+    timings = head["timings"]
     stage = {k: float(np.mean([t[k] for t in timings])) for k in
              ("lag_ms", "spectrogram_ms", "prep_ms", "nsim_ms", "realign_ms", "gammatone_kernel_ms", "total_ms")}
 
@@ -258,38 +291,44 @@ def run_ours(args, rank, world, local):
     plain = []
     for i in range(min(4, B)):
         t0 = time.perf_counter()
-        o = ctx.measure(pin_r[i], pin_d[i], 48000)
+        o = ctxs["exact"].measure(pin_r[i], pin_d[i], 48000)
         native.free(o)
         plain.append(time.perf_counter() - t0)
+    plain_value = 1.0 / float(np.mean(plain))
 
+    walls = head["walls"]
     line = {
-        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRICS[args.precision], "value": head["value"], "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
         "config": {"workload": WORKLOAD, "batch_per_gpu": B, "global_batch": world * B,
                    "inputs": "device-resident for value; pinned host for e2e",
-                   "l2": "inputs (~0.5 GB per step) exceed L2; no flush", "precision": "exact"},
+                   "l2": "inputs (~0.5 GB per step) exceed L2; no flush", "precision": args.precision},
         "latency_ms": {"batch_p50": 1e3 * float(np.percentile(walls, 50)),
                        "batch_p99": 1e3 * float(np.percentile(walls, 99)),
                        "plain_single_pair_p50": 1e3 * float(np.percentile(plain, 50))},
-        "plain_exact_pairs_per_s": 1.0 / float(np.mean(plain)),
+        "plain_exact_pairs_per_s": plain_value,
+        "speedup_vs_plain_exact": head["value"] / plain_value,
         "stage_ms": stage,
-        "roofline": {"bound": "fp64-pipe", "kernel": "gammatone_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": (achieved / peak) if achieved and peak else None,
-                     "traffic": traffic, "peak_source": "measured here: f64 mul+add pipe (visqol_b200_peak kind 0)",
-                     "flops_per_rms": 31 * window},
+        "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "signal_bytes_per_step": int(signal_bytes)},
         "gpu_launches": int(sum(t["kernel_launches"] for t in timings)),
-        "clocks": clocks.summary(),
-        "failures": failures,
+        "clocks": head["clocks"],
+        "failures": head["failures"],
+        "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline": r["roofline"],
+                      "failures": r["failures"]} for f, r in runs.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pairs, args.seconds)
         res = cb.pop("results")
-        dmos = [abs(r["moslqo"] - g[1]["moslqo"]) for (c, r), g in zip(res, results) if c == 0 and g[0] == 0]
         line["cpu_baseline"] = cb
-        line["parity"] = {"pairs": len(dmos), "max_abs_dmos_vs_oracle": max(dmos) if dmos else None}
+        for f, r in runs.items():
+            dmos = [abs(o["moslqo"] - g[1]["moslqo"]) for (c, o), g in zip(res, r["results"]) if c == 0 and g[0] == 0]
+            line["forms"][f]["max_abs_dmos_vs_oracle"] = max(dmos) if dmos else None
+            line["forms"][f]["parity_pairs"] = len(dmos)
+        line["parity"] = {"pairs": line["forms"][args.precision]["parity_pairs"],
+                          "max_abs_dmos_vs_oracle": line["forms"][args.precision]["max_abs_dmos_vs_oracle"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -1,0 +1,82 @@
+"""The two fast arithmetic forms against the oracle (the exact CPU path).
+
+* balanced: f64 with FMA (direct-form-I gammatone) and tree-summed
+  statistics. It reorders rounding only, so MOS stays within 1e-10 and
+  every discrete decision (lags, patch indices, DP offsets, realignment)
+  matches.
+* fast: gammatone stages 2-4 in f32. MOS within 1e-6 on the 10 s 48 kHz
+  audio workload; on low-SNR pairs whose upper bands hold flat white noise
+  NSIM's structure term amplifies f32 rounding, and the stated bound there is
+  1e-5. Lags, patch indices (VAD in speech mode) and matched offsets must
+  still be identical.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DISCRETE = ("ref_index", "deg_offset", "valid", "realign_lag", "realign_frames", "realign_reused",
+            "realign_accepted")
+
+
+def run(ctx, pairs, sr):
+    return ctx.measure_batch_traced([p[0] for p in pairs], [p[1] for p in pairs], sr)
+
+
+def check(got, pairs, sr, oracle, opts, mos_tol):
+    worst = 0.0
+    for (code, res, tr), (ref, deg) in zip(got, pairs):
+        assert code == 0
+        want, wtr = oracle.measure(ref, deg, sr, opts)
+        d = abs(res["moslqo"] - want["moslqo"])
+        worst = max(worst, d)
+        assert d <= mos_tol, d
+        assert tr["global_lag"] == wtr["global_lag"]
+        assert abs(tr["spl_factor"] - wtr["spl_factor"]) <= 1e-12 * abs(wtr["spl_factor"])
+        for key in ("deg_len", "nf_ref", "nf_deg", "num_patches"):
+            assert tr[key] == wtr[key], key
+        for key in DISCRETE:
+            assert np.array_equal(tr[key], wtr[key]), key
+    return worst
+
+
+@pytest.fixture(scope="module")
+def contexts(native):
+    return {(form, mode): native.Context(mode=mode, use_lattice_model=False, precision=form)
+            for form in ("balanced", "fast") for mode in (native.MODE_AUDIO, native.MODE_SPEECH)}
+
+
+@pytest.mark.parametrize("form,tol", [("balanced", 1e-10), ("fast", 1e-6)])
+def test_audio_10s_48k(native, oracle, contexts, form, tol):
+    from akvisqol_b200 import synth
+    pairs = [synth.audio_pair(synth.SEED_BASE + i) for i in range(4)]
+    check(run(contexts[(form, native.MODE_AUDIO)], pairs, 48000), pairs, 48000, oracle, oracle.options(), tol)
+
+
+@pytest.mark.parametrize("form,tol", [("balanced", 1e-10), ("fast", 1e-5)])
+def test_uneven_audio(native, oracle, contexts, form, tol):
+    from akvisqol_b200 import synth
+    pairs = synth.audio_batch(8, min_s=3.0, max_s=8.0)
+    check(run(contexts[(form, native.MODE_AUDIO)], pairs, 48000), pairs, 48000, oracle, oracle.options(), tol)
+
+
+@pytest.mark.parametrize("form,tol", [("balanced", 1e-10), ("fast", 1e-6)])
+def test_speech(native, oracle, contexts, form, tol):
+    from akvisqol_b200 import synth
+    pairs = synth.speech_batch(8, min_s=2.0, max_s=8.0)
+    check(run(contexts[(form, native.MODE_SPEECH)], pairs, 16000), pairs, 16000, oracle, oracle.options(mode=1), tol)
+
+
+@pytest.mark.parametrize("form", ["balanced", "fast"])
+def test_batch_equals_single(native, contexts, form):
+    """Deterministic: a pair scores the same alone and inside a batch."""
+    from akvisqol_b200 import synth
+    pairs = synth.audio_batch(5, min_s=3.0, max_s=6.0)
+    ctx = contexts[(form, native.MODE_AUDIO)]
+    batch = run(ctx, pairs, 48000)
+    for (code, res, _), p in zip(batch, pairs):
+        (code1, res1, _), = run(ctx, [p], 48000)
+        assert code == code1 == 0
+        assert res["moslqo"] == res1["moslqo"]
+        assert np.array_equal(res["fvnsim"], res1["fvnsim"])
