@@ -20,6 +20,7 @@
 
 #include "../../include/visqol.h"
 #include "../../include/visqol_b200.h"
+#include "capi_internal.h"
 #include "engine.h"
 #include "host_model.h"
 
@@ -50,6 +51,8 @@ int fail(int code, const std::string &m) {
     return code;
 }
 
+}  // namespace
+
 // A result and the storage its pointers view (reference src/capi.zig:66-70).
 struct Box {
     visqol_result c{};
@@ -58,7 +61,7 @@ struct Box {
     std::vector<visqol_patch> patches;
 };
 
-visqol_result *box_scores(vqb::host::Scores &&s) {
+visqol_result *vqb::box_result(vqb::host::Scores &&s) {
     auto *b = new Box();
     b->s = std::move(s);
     const size_t nb = b->s.fvnsim.size(), np = b->s.patches.size();
@@ -86,6 +89,8 @@ visqol_result *box_scores(vqb::host::Scores &&s) {
     b->c.patch_sims = b->patches.data();
     return &b->c;
 }
+
+namespace {
 
 struct TraceBox {
     visqol_b200_trace c{};
@@ -217,7 +222,7 @@ int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *
         if (traces) traces[i] = nullptr;
         int rc = res[i].code;
         if (rc == VISQOL_OK) {
-            out[i] = box_scores(std::move(res[i].scores));
+            out[i] = vqb::box_result(std::move(res[i].scores));
             if (traces) traces[i] = box_trace(std::move(res[i].trace));
         } else {
             set_error(res[i].message);
@@ -238,6 +243,55 @@ int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *
 }  // namespace
 
 void vqb::set_last_error(const std::string &message) { set_error(message); }
+
+int vqb::engine_options(const visqol_options &o, Options *opt, std::shared_ptr<const host::Svr> *svr,
+                        std::string *message) {
+    // EXACT (and AUTO, which resolves to exact on a device with native f64)
+    // reproduce the CPU path; FAST runs the gammatone's later stages in f32;
+    // BALANCED keeps f64 throughout but with FMA and reassociated sums.
+    opt->form = o.precision == VISQOL_PRECISION_FAST       ? kFormF32
+                : o.precision == VISQOL_PRECISION_BALANCED ? kFormF64
+                                                           : kFormExact;
+    opt->speech = o.mode == VISQOL_MODE_SPEECH;
+    opt->radius = o.search_window_radius > 0 ? o.search_window_radius : 60;
+    opt->unscaled_speech = o.use_unscaled_speech_mos_mapping != 0;
+    opt->disable_global_alignment = o.disable_global_alignment != 0;
+    opt->disable_realignment = o.disable_realignment != 0;
+    if (opt->speech && o.use_lattice_model) {
+        *message = "UnsupportedOp: the TF-Lattice speech mapper is not in this build; "
+                   "set use_lattice_model = 0 for the exponential mapping";
+        return VISQOL_E_MODEL;
+    }
+    if (!opt->speech) {
+        const std::string text =
+            (o.model_path && o.model_path[0]) ? host::read_file(o.model_path) : host::default_svr_text();
+        *svr = std::make_shared<host::Svr>(host::parse_svr(text));
+    }
+    return VISQOL_OK;
+}
+
+int vqb::context_device(int *device, std::string *message) {
+    const int ndev = device_count();
+    if (ndev == 0) {
+        *message = "BackendUnavailable: no CUDA device";
+        return VISQOL_E_BACKEND;
+    }
+    // VISQOL_CUDA_DEVICE picks the GPU (one process per GPU); else device 0.
+    int dev = 0;
+    if (const char *env = std::getenv("VISQOL_CUDA_DEVICE")) dev = std::atoi(env);
+    if (dev < 0 || dev >= ndev) {
+        *message = "VISQOL_CUDA_DEVICE out of range";
+        return VISQOL_E_INVALID_ARGUMENT;
+    }
+    *device = dev;
+    return VISQOL_OK;
+}
+
+int vqb::env_lanes(int fallback) {
+    int lanes = fallback;
+    if (const char *env = std::getenv("VISQOL_GPU_LANES")) lanes = std::atoi(env);
+    return std::max(1, std::min(lanes, 8));
+}
 
 extern "C" {
 
@@ -275,35 +329,12 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
     if (o.backend != VISQOL_BACKEND_CUDA)
         return fail(VISQOL_E_BACKEND, "BackendUnavailable: this libvisqol serves backend cuda (2) only");
     auto c = std::make_unique<visqol_ctx>();
-    // EXACT (and AUTO, which resolves to exact on a device with native f64)
-    // reproduce the CPU path; FAST runs the gammatone's later stages in f32;
-    // BALANCED keeps f64 throughout but with FMA and reassociated sums.
-    c->opt.form = o.precision == VISQOL_PRECISION_FAST       ? vqb::kFormF32
-                  : o.precision == VISQOL_PRECISION_BALANCED ? vqb::kFormF64
-                                                             : vqb::kFormExact;
-    c->opt.speech = o.mode == VISQOL_MODE_SPEECH;
-    c->opt.radius = o.search_window_radius > 0 ? o.search_window_radius : 60;
-    c->opt.unscaled_speech = o.use_unscaled_speech_mos_mapping != 0;
-    c->opt.disable_global_alignment = o.disable_global_alignment != 0;
-    c->opt.disable_realignment = o.disable_realignment != 0;
     try {
-        if (c->opt.speech && o.use_lattice_model)
-            return fail(VISQOL_E_MODEL, "UnsupportedOp: the TF-Lattice speech mapper is not in this build; "
-                                        "set use_lattice_model = 0 for the exponential mapping");
-        if (!c->opt.speech) {
-            const std::string text = (o.model_path && o.model_path[0]) ? vqb::host::read_file(o.model_path)
-                                                                       : vqb::host::default_svr_text();
-            c->svr = std::make_shared<vqb::host::Svr>(vqb::host::parse_svr(text));
-        }
-        const int ndev = device_count();
-        if (ndev == 0) return fail(VISQOL_E_BACKEND, "BackendUnavailable: no CUDA device");
-        // VISQOL_CUDA_DEVICE picks the GPU (one process per GPU); else device 0.
+        std::string msg;
+        if (int rc = vqb::engine_options(o, &c->opt, &c->svr, &msg)) return fail(rc, msg);
         int dev = 0;
-        if (const char *env = std::getenv("VISQOL_CUDA_DEVICE")) dev = std::atoi(env);
-        if (dev < 0 || dev >= ndev) return fail(VISQOL_E_INVALID_ARGUMENT, "VISQOL_CUDA_DEVICE out of range");
-        int lanes = 2;
-        if (const char *env = std::getenv("VISQOL_GPU_LANES")) lanes = std::atoi(env);
-        lanes = std::max(1, std::min(lanes, 8));
+        if (int rc = vqb::context_device(&dev, &msg)) return fail(rc, msg);
+        const int lanes = vqb::env_lanes(2);
         for (int l = 0; l < lanes; ++l) c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr));
     } catch (const Error &e) {
         return fail(e.code, e.what());

@@ -157,12 +157,18 @@ const Engine::RateCache &Engine::rate_cache(uint32_t sr) {
     const std::vector<double> w = host::hann(rc.geo.window);
     VQB_CUDA(cudaMalloc(&rc.d_coeffs, nb_ * sizeof(BandCoeffs)));
     VQB_CUDA(cudaMalloc(&rc.d_hann, std::max<size_t>(1, w.size()) * sizeof(double)));
-    VQB_CUDA(cudaMemcpy(rc.d_coeffs, rc.fb.run.data(), nb_ * sizeof(BandCoeffs), cudaMemcpyHostToDevice));
+    // Copies from pageable memory are ordered on this engine's stream (a
+    // plain cudaMemcpy may return before its DMA lands, and the engine's
+    // non-blocking streams would not wait for it).
     std::vector<FastBandCoeffs> fast(nb_);
     fill_fast_band_coeffs(rc.fb.run.data(), rc.fb.cf.data(), (int)nb_, fast.data());
     VQB_CUDA(cudaMalloc(&rc.d_fast_coeffs, nb_ * sizeof(FastBandCoeffs)));
-    VQB_CUDA(cudaMemcpy(rc.d_fast_coeffs, fast.data(), nb_ * sizeof(FastBandCoeffs), cudaMemcpyHostToDevice));
-    if (!w.empty()) VQB_CUDA(cudaMemcpy(rc.d_hann, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+    VQB_CUDA(cudaMemcpyAsync(rc.d_coeffs, rc.fb.run.data(), nb_ * sizeof(BandCoeffs), cudaMemcpyHostToDevice, stream_));
+    VQB_CUDA(cudaMemcpyAsync(rc.d_fast_coeffs, fast.data(), nb_ * sizeof(FastBandCoeffs), cudaMemcpyHostToDevice,
+                             stream_));
+    if (!w.empty())
+        VQB_CUDA(cudaMemcpyAsync(rc.d_hann, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    VQB_CUDA(cudaStreamSynchronize(stream_));
     return rates_.emplace(sr, std::move(rc)).first->second;
 }
 
@@ -177,10 +183,19 @@ Engine::Twiddles Engine::twiddles(size_t n) {
     const size_t cols_at = t.size();
     t.resize(cols_at + column_twiddle_count((int64_t)n));
     fill_column_twiddles(t.data(), (int64_t)n, t.data() + cols_at);
+    // the 4096-point block stages' stage-major table (fused search, n > 4096)
+    const size_t stages_at = t.size();
+    if (B == 4096) {
+        t.resize(stages_at + block_stage_twiddle_count());
+        fill_block_stage_twiddles(t.data() + half, t.data() + stages_at);
+    }
     double2 *d = nullptr;
     VQB_CUDA(cudaMalloc(&d, std::max<size_t>(1, t.size()) * sizeof(double2)));
-    if (!t.empty()) VQB_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
-    Twiddles tw{d, d + half, d + cols_at};
+    if (!t.empty()) {
+        VQB_CUDA(cudaMemcpyAsync(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, stream_));
+        VQB_CUDA(cudaStreamSynchronize(stream_));
+    }
+    Twiddles tw{d, d + half, d + cols_at, d + stages_at};
     twiddles_[n] = tw;
     return tw;
 }
@@ -242,7 +257,7 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
                 const size_t parts = fused_lag_parts(n);
                 double *pv = arena_.alloc_n<double>(parts * cnt);
                 int64_t *pk = arena_.alloc_n<int64_t>(parts * cnt);
-                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, pv, pk, stream_);
+                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, tw.stages, pv, pk, stream_);
                 continue;
             }
             const int parts = argmax_parts(n);
@@ -255,6 +270,25 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
             launch_argmax(z, d_jobs, (int)cnt, n, n, pv, pk, stream_);
         }
     }
+}
+
+size_t Engine::pair_footprint(size_t rl, size_t dl, uint32_t sample_rate, bool speech) {
+    const size_t H = std::max<size_t>(1, host::analysis_geometry(sample_rate).hop);
+    const size_t NB = speech ? 21 : 32, P = speech ? 20 : 30;
+    const size_t al = dl + rl / 2 + 1;  // aligned degraded length bound (|lag| <= ref/2)
+    const size_t nfr = rl / H + 1, nfd = al / H + 1;
+    const size_t width = nfd + 2 * P + 2;
+    const size_t np = nfr / std::max<size_t>(1, P) + 1;
+    const size_t n_global = host::fft_size_for(std::max(rl, dl));
+    const size_t n_slice = host::fft_size_for(2 * P * H + 2);
+    size_t b = 8 * (rl + dl)                                   // inputs
+               + 16 * n_global + 16 * 1024                     // lag search and argmax parts
+               + 8 * al                                        // aligned, scaled degraded signal
+               + 8 * NB * (2 * nfr + 2 * nfd + 4 * width)      // spectrograms, prepared copies, plane
+               + np * (8 * 4 * NB * P + 24 * nfd + 8 * (3 * NB + 1) + 16)  // terms, table, DP, stats
+               + np * (16 * n_slice + 8 * 4 * NB * (2 * P + 2) + 256);     // realignment slices
+    b += b / 4 + (size_t(1) << 20);  // job tables, tiles, rounding slack
+    return b;
 }
 
 void Engine::launch_sums(const std::vector<SumJob> &sums) {
@@ -627,7 +661,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     record(events_[4]);
     if (!plane_jobs.empty()) launch_plane(upload(plane_jobs), (int)plane_jobs.size(), nbi, max_width, stream_);
     if (!term_jobs.empty()) launch_ref_terms(upload(term_jobs), (int)term_jobs.size(), nbi, (int)P, stream_);
-    if (!tasks.empty()) launch_table(upload(tasks), (int)tasks.size(), nbi, (int)P, stream_);
+    if (!tasks.empty()) launch_table(upload(tasks), (int)tasks.size(), nbi, (int)P, opt_.form != kFormExact, stream_);
     if (!dp_jobs.empty()) launch_dp(upload(dp_jobs), (int)dp_jobs.size(), stream_);
     if (!stat_jobs.empty()) launch_stats(upload(stat_jobs), (int)stat_jobs.size(), nbi, stream_);
     std::vector<int64_t *> h_offs(n, nullptr);

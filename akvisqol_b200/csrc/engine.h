@@ -105,6 +105,11 @@ public:
                        std::vector<PairOutcome> &out);
 
     const Timing &last_timing() const { return timing_; }
+    // Upper bound on the device memory one pair of these lengths takes in
+    // measure_batch (host inputs included), for admission by footprint.
+    static size_t pair_footprint(size_t ref_len, size_t deg_len, uint32_t sample_rate, bool speech);
+    // Device memory the engine holds now (arena chunks).
+    size_t reserved_bytes() const { return arena_.reserved(); }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
 
@@ -115,7 +120,7 @@ public:
     // FFT twiddles of size n on the device: the full table and the block
     // passes' compact one (cached per size).
     struct Twiddles {
-        const double2 *top, *block, *cols;
+        const double2 *top, *block, *cols, *stages;
     };
     Twiddles twiddles(size_t n);
 

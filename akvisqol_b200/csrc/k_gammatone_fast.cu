@@ -77,8 +77,24 @@ __device__ inline float2 stage32(float2 v, F32Stage &s, float2 beta, float2 np1h
     return y;
 }
 
-template <bool kDirectI>
-__device__ void band_frames(const VSig &sig, int64_t ka, int64_t kb, const FastBandCoeffs &k,
+// Samples of a frame: straight loads when the whole window lies inside the
+// signal's stored samples (nearly every frame), else VSig's bounds-checked
+// view (zero padding at slice edges).
+struct Direct {
+    const double *p;
+    __device__ double operator()(int64_t k) const { return p[k]; }
+};
+struct Checked {
+    VSig s;
+    __device__ double operator()(int64_t k) const { return vsig_at(s, k); }
+};
+
+__device__ inline bool window_inside(const VSig &sig, int64_t k0, int64_t span) {
+    return k0 - sig.head >= 0 && k0 + span - sig.head <= sig.avail;
+}
+
+template <bool kDirectI, class Load>
+__device__ void band_frames(const Load &sample, int64_t ka, int64_t kb, const FastBandCoeffs &k,
                             const double *__restrict__ hann, int window, double &acc_a, double &acc_b) {
     double c0a = 0.0, c1a = 0.0, c0b = 0.0, c1b = 0.0;
     F32Stage st[3];
@@ -91,8 +107,8 @@ __device__ void band_frames(const VSig &sig, int64_t ka, int64_t kb, const FastB
     acc_b = 0.0;
     auto step = [&](int i, float2 &part) {
         const double h = __ldg(hann + i);
-        const double xa = vsig_at(sig, ka + i) * h;
-        const double xb = vsig_at(sig, kb + i) * h;
+        const double xa = sample(ka + i) * h;
+        const double xb = sample(kb + i) * h;
         const double fa = __fma_rn(n0, xa, c0a);
         const double fb = __fma_rn(n0, xb, c0b);
         c0a = __fma_rn(nd1, fa, __fma_rn(n1, xa, c1a));
@@ -134,38 +150,36 @@ __global__ void __launch_bounds__(256) gammatone_fast_kernel(const SpecJob *__re
     const FastBandCoeffs k = coeffs[band];
     const int64_t ka = f * hop, kb = ka + hop;
     double acc_a, acc_b;
-    if (k.direct_i)
-        band_frames<true>(job.sig, ka, kb, k, hann, window, acc_a, acc_b);
-    else
-        band_frames<false>(job.sig, ka, kb, k, hann, window, acc_a, acc_b);
+    const VSig &sig = job.sig;
+    if (window_inside(sig, ka, hop + window)) {
+        const Direct ld{sig.base - sig.head};
+        if (k.direct_i)
+            band_frames<true>(ld, ka, kb, k, hann, window, acc_a, acc_b);
+        else
+            band_frames<false>(ld, ka, kb, k, hann, window, acc_a, acc_b);
+    } else {
+        const Checked ld{sig};
+        if (k.direct_i)
+            band_frames<true>(ld, ka, kb, k, hann, window, acc_a, acc_b);
+        else
+            band_frames<false>(ld, ka, kb, k, hann, window, acc_a, acc_b);
+    }
     const double inv_n = 1.0 / (double)window;
     double *out = job.out + (int64_t)band * job.nf;
     out[f] = sqrt(acc_a * inv_n) * k.post;
     if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post;
 }
 
-__global__ void __launch_bounds__(256) gammatone_f64fma_kernel(const SpecJob *__restrict__ jobs,
-                                                               const Tile *__restrict__ tiles,
-                                                               const FastBandCoeffs *__restrict__ coeffs, int nb,
-                                                               const double *__restrict__ hann, int window, int hop) {
-    const Tile tile = tiles[blockIdx.x];
-    const int frames_per_cta = blockDim.x / nb;
-    const int fl = threadIdx.x / nb;
-    const int band = threadIdx.x - fl * nb;
-    if (fl >= frames_per_cta) return;
-    const SpecJob job = jobs[tile.job];
-    const int64_t f = (int64_t)tile.frame0 + fl;
-    if (f >= job.nf) return;
-    const FastBandCoeffs &kc = coeffs[band];
+template <class Load>
+__device__ double cascade64(const Load &sample, int64_t k0, const FastBandCoeffs &kc, const double *__restrict__ hann,
+                            int window) {
     const double b0 = kc.beta64[0], b1 = kc.beta64[1], b2 = kc.beta64[2], b3 = kc.beta64[3];
     const double nd1 = -kc.d1, nd2 = -kc.d2;
     double xp = 0.0, y1a = 0.0, y2a = 0.0, y1b = 0.0, y2b = 0.0, y1c = 0.0, y2c = 0.0, y1d = 0.0, y2d = 0.0;
     double acc = 0.0;
-    const int64_t k0 = f * hop;
-    const VSig sig = job.sig;
 #pragma unroll 4
     for (int i = 0; i < window; ++i) {
-        const double x = vsig_at(sig, k0 + i) * __ldg(hann + i);
+        const double x = sample(k0 + i) * __ldg(hann + i);
         // stage k input v, previous input vp = stage k-1's previous output
         const double ya = __fma_rn(nd1, y1a, __fma_rn(nd2, y2a, __fma_rn(b0, xp, x)));
         const double yb = __fma_rn(nd1, y1b, __fma_rn(nd2, y2b, __fma_rn(b1, y1a, ya)));
@@ -182,9 +196,33 @@ __global__ void __launch_bounds__(256) gammatone_f64fma_kernel(const SpecJob *__
         y1d = yd;
         acc = __fma_rn(yd, yd, acc);
     }
+    return acc;
+}
+
+__global__ void __launch_bounds__(256) gammatone_f64fma_kernel(const SpecJob *__restrict__ jobs,
+                                                               const Tile *__restrict__ tiles,
+                                                               const FastBandCoeffs *__restrict__ coeffs, int nb,
+                                                               const double *__restrict__ hann, int window, int hop) {
+    const Tile tile = tiles[blockIdx.x];
+    const int frames_per_cta = blockDim.x / nb;
+    const int fl = threadIdx.x / nb;
+    const int band = threadIdx.x - fl * nb;
+    if (fl >= frames_per_cta) return;
+    const SpecJob job = jobs[tile.job];
+    const int64_t f = (int64_t)tile.frame0 + fl;
+    if (f >= job.nf) return;
+    const FastBandCoeffs &kc = coeffs[band];
+    const int64_t k0 = f * hop;
+    const VSig sig = job.sig;
+    double acc;
+    if (window_inside(sig, k0, window))
+        acc = cascade64(Direct{sig.base - sig.head}, k0, kc, hann, window);
+    else
+        acc = cascade64(Checked{sig}, k0, kc, hann, window);
     const double inv_n = 1.0 / (double)window;
     job.out[(int64_t)band * job.nf + f] = sqrt(acc * inv_n) * kc.post64;
 }
+
 
 }  // namespace
 

@@ -317,11 +317,63 @@ __device__ inline void blocks_dit(double2 *s0, double2 *s1, int B, const double2
     }
 }
 
-// Pass 2. CTA 0: block 0 (partners inside it, reference pairing
+// Pass 2 on the 4096-point blocks, in registers: each radix-2 stage group of
+// four (spans S0 .. S0/8) runs on 16 points per thread (point j + m*S0/16 of
+// an S0-block, m = 0..15), so the 12 DIF stages, the cross terms and the 12
+// DIT stages take three register passes each way with four shared-memory
+// round trips in all (the first and last passes read and write global
+// memory directly). Shared memory holds the two blocks padded by one point
+// per 16 (position e at e + e/16), which keeps all three access patterns
+// (stride 256, 16 and 1 points) free of bank conflicts. Twiddles come from
+// the stage-major table tst[(4096 - S) + k] = W_S^k, contiguous per stage.
+//
+// CTA 0: block 0 (partners inside it, reference pairing
 // src/xcorr.zig:211-229); CTA 1: block 1 (u <-> B-1-u); CTA k >= 2: blocks
 // b and b' = 3*hb - 1 - b for the (k-1)-th pair, hb = 2 * floor_pow2(k-1).
-__global__ void __launch_bounds__(2 * kThreads) middle_blocks(const LagJob *__restrict__ jobs, int B,
-                                                          const double2 *__restrict__ tw) {
+// Threads 0..255 own the first block, 256..511 the second.
+constexpr int kMidThreads = 512;
+constexpr int kPadB = kB + kB / 16;
+
+__device__ inline int padi(int e) { return e + (e >> 4); }
+
+template <int S0>
+__device__ inline void dif16(double2 (&x)[16], int j, const double2 *__restrict__ tst) {
+    constexpr int q = S0 / 16;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int half = 8 >> r;
+        const double2 *tw = tst + (kB - (S0 >> r));
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & half) continue;
+            const double2 w = __ldg(tw + j + (m & (half - 1)) * q);
+            const double2 a = x[m], b = x[m + half];
+            x[m] = cadd(a, b);
+            x[m + half] = cmul(csub(a, b), w);
+        }
+    }
+}
+
+template <int S0>
+__device__ inline void dit16(double2 (&x)[16], int j, const double2 *__restrict__ tst) {
+    constexpr int q = S0 / 16;
+#pragma unroll
+    for (int r = 3; r >= 0; --r) {
+        const int half = 8 >> r;
+        const double2 *tw = tst + (kB - (S0 >> r));
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & half) continue;
+            const double2 w = __ldg(tw + j + (m & (half - 1)) * q);
+            const double2 a = x[m], b = cmul_conj(x[m + half], w);
+            x[m] = cadd(a, b);
+            x[m + half] = csub(a, b);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__restrict__ jobs,
+                                                                const double2 *__restrict__ tst) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
     const int k = blockIdx.x;
@@ -335,48 +387,82 @@ __global__ void __launch_bounds__(2 * kThreads) middle_blocks(const LagJob *__re
         b0 = i + p;
         b1 = 3 * hb - 1 - b0;
     }
-    double2 *s0 = sm, *s1 = b1 >= 0 ? sm + B : nullptr;
-    double2 *z0 = job.z + b0 * B, *z1 = b1 >= 0 ? job.z + b1 * B : nullptr;
-    for (int u = threadIdx.x; u < B; u += blockDim.x) {
-        s0[u] = z0[u];
-        if (s1) s1[u] = z1[u];
+    const int half = threadIdx.x >> 8, t = threadIdx.x & 255;
+    const bool active = half == 0 || b1 >= 0;
+    double2 *own = sm + half * kPadB;
+    double2 *z = job.z + (half == 1 && b1 >= 0 ? b1 : b0) * kB;
+    double2 x[16];
+    // DIF spans 4096 .. 512: points t + 256 m
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = z[t + 256 * m];
+        dif16<4096>(x, t, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) own[padi(t + 256 * m)] = x[m];
     }
     __syncthreads();
-    blocks_dif(s0, s1, B, tw);
-    if (s1) {
-        for (int u = threadIdx.x; u < B; u += blockDim.x) {
-            const double2 za = s0[u], zb = s1[B - 1 - u];
-            s0[u] = cross_term(za, zb);
-            s1[B - 1 - u] = cross_term(zb, za);
-        }
-    } else if (k == 1) {
-        for (int u = threadIdx.x; u < B / 2; u += blockDim.x) {
-            const double2 za = s0[u], zb = s0[B - 1 - u];
-            s0[u] = cross_term(za, zb);
-            s0[B - 1 - u] = cross_term(zb, za);
-        }
-    } else {
-        // block 0: positions 0 and 1 pair with themselves; position a in
-        // [h, 2h) with 3h-1-a.
-        for (int i = threadIdx.x; i < (B > 1 ? B / 2 : 1); i += blockDim.x) {
-            if (i == 0) {
-                s0[0] = cross_term(s0[0], s0[0]);
-                if (B > 1) s0[1] = cross_term(s0[1], s0[1]);
-                continue;
+    // DIF spans 256 .. 32: points (t/16)*256 + t%16 + 16 m
+    const int base2 = (t >> 4) * 256 + (t & 15);
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = own[padi(base2 + 16 * m)];
+        dif16<256>(x, t & 15, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) own[padi(base2 + 16 * m)] = x[m];
+    }
+    __syncthreads();
+    // DIF spans 16 .. 2: points 16 t + m
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = own[padi(16 * t + m)];
+        dif16<16>(x, 0, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) own[padi(16 * t + m)] = x[m];
+    }
+    __syncthreads();
+    // cross terms: each point with its partner's forward value
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int u = 16 * t + m;
+            double2 zp;
+            if (b1 >= 0) {
+                zp = sm[(1 - half) * kPadB + padi(kB - 1 - u)];
+            } else if (k == 1) {
+                zp = own[padi(kB - 1 - u)];
+            } else {
+                int p = u;
+                if (u >= 2) {
+                    const int h = 1 << (31 - __clz(u));
+                    p = 3 * h - 1 - u;
+                }
+                zp = own[padi(p)];
             }
-            const int p = 1 << (31 - __clz(i));
-            const int h = 2 * p;
-            const int a = i + p, b = 3 * h - 1 - a;
-            const double2 za = s0[a], zb = s0[b];
-            s0[a] = cross_term(za, zb);
-            s0[b] = cross_term(zb, za);
+            x[m] = cross_term(x[m], zp);
         }
     }
     __syncthreads();
-    blocks_dit(s0, s1, B, tw);
-    for (int u = threadIdx.x; u < B; u += blockDim.x) {
-        z0[u] = s0[u];
-        if (s1) z1[u] = s1[u];
+    // DIT spans 2 .. 16, then 32 .. 256, then 512 .. 4096 (to global memory)
+    if (active) {
+        dit16<16>(x, 0, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) own[padi(16 * t + m)] = x[m];
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = own[padi(base2 + 16 * m)];
+        dit16<256>(x, t & 15, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) own[padi(base2 + 16 * m)] = x[m];
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = own[padi(t + 256 * m)];
+        dit16<4096>(x, t, tst);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) z[t + 256 * m] = x[m];
     }
 }
 
@@ -485,13 +571,14 @@ __global__ void pick_lag(const LagJob *__restrict__ jobs, int njobs, const doubl
 }  // namespace
 
 void lag_init_attributes() {
-    const int one = kB * (int)sizeof(double2), two = 2 * one;
+    const int one = kB * (int)sizeof(double2);
     cudaFuncSetAttribute(fwd_columns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(fwd_columns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(inv_columns_argmax, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(small_lag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(small_lag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
-    cudaFuncSetAttribute(middle_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, two);
+    cudaFuncSetAttribute(middle_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(2 * kPadB * sizeof(double2)));
 }
 
 bool fused_lag_supported(int64_t n) { return n >= 1 && n <= ((int64_t)kB << 12); }
@@ -506,6 +593,14 @@ size_t fused_lag_parts(int64_t n) {
 
 size_t column_twiddle_count(int64_t n) { return n <= kB ? 0 : (size_t)(n - kB); }
 
+size_t block_stage_twiddle_count() { return kB - 1; }
+
+void fill_block_stage_twiddles(const double2 *block, double2 *out) {
+    // out[(4096 - S) + k] = W_S^k = block[k * 4096 / S], spans S = 4096 .. 2
+    for (int S = kB; S >= 2; S >>= 1)
+        for (int k2 = 0; k2 < S / 2; ++k2) out[(kB - S) + k2] = block[(size_t)k2 * (kB / S)];
+}
+
 void fill_column_twiddles(const double2 *top, int64_t n, double2 *out) {
     if (n <= kB) return;
     int G = 0;
@@ -518,7 +613,7 @@ void fill_column_twiddles(const double2 *top, int64_t n, double2 *out) {
 }
 
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
-                      const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s) {
+                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, cudaStream_t s) {
     if (njobs <= 0) return;
     const size_t one = (size_t)kB * sizeof(double2);
     if (n <= kB) {
@@ -539,8 +634,8 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
         fwd_columns<true><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
     else
         fwd_columns<false><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
-    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), 2 * kThreads, 2 * one, s>>>(d_jobs, kB,
-                                                                                                tw_block);
+    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads, 2 * kPadB * sizeof(double2), s>>>(
+        d_jobs, tst);
     inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);
     pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
     launch_counter() += 4;

@@ -105,8 +105,12 @@ size_t fused_lag_parts(int64_t n);  // argmax candidates per job
 // full table top[k] = W_n^k): column_twiddle_count(n) entries.
 size_t column_twiddle_count(int64_t n);
 void fill_column_twiddles(const double2 *top, int64_t n, double2 *out);
+// Stage-major twiddles of the 4096-point block stages, from the block table
+// (block[k] = W_4096^k): block_stage_twiddle_count() entries.
+size_t block_stage_twiddle_count();
+void fill_block_stage_twiddles(const double2 *block, double2 *out);
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
-                      const double2 *tw_block, double *pv, int64_t *pk, cudaStream_t s);
+                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, cudaStream_t s);
 
 // k_gammatone.cu
 int gammatone_frames_per_cta(int nb);
@@ -134,7 +138,8 @@ void nsim_init_attributes();
 void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cudaStream_t s);
 void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaStream_t s);
 int table_offsets_per_cta();
-void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, cudaStream_t s);
+// fast: the fast forms' cell arithmetic (FMA, one division per cell).
+void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, cudaStream_t s);
 void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s);
 
 // k_dp.cu

@@ -28,7 +28,12 @@ struct DBuf {
     T *p = nullptr;
     explicit DBuf(size_t n) { VQB_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T))); }
     DBuf(const T *h, size_t n) : DBuf(n) {
-        if (n) VQB_CUDA(cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+        // A copy from pageable memory may return before its DMA lands; the
+        // kernels run on a non-blocking stream, so wait for it.
+        if (n) {
+            VQB_CUDA(cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+            VQB_CUDA(cudaDeviceSynchronize());
+        }
     }
     ~DBuf() { cudaFree(p); }
     void get(T *h, size_t n) const {
@@ -155,7 +160,7 @@ int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref, const double *
         for (size_t p = 0; p < np; ++p) width = std::max(width, (size_t)hi[p] + patch);
         DBuf<double> rs(ref_spec, nb * nf_ref), ds(deg_spec, nb * nf_deg), plane(4 * nb * width),
             terms(np * 4 * nb * patch), sims(np * nf_deg);
-        VQB_CUDA(cudaMemset(sims.p, 0, std::max<size_t>(1, np * nf_deg) * sizeof(double)));
+        VQB_CUDA(cudaMemsetAsync(sims.p, 0, std::max<size_t>(1, np * nf_deg) * sizeof(double), e.stream()));
         const size_t pl = nb * width;
         vqb::PlaneJob pj{ds.p, (int32_t)nf_deg, (int32_t)width, plane.p, plane.p + pl, plane.p + 2 * pl, plane.p + 3 * pl};
         std::vector<vqb::RefTermsJob> tj;
@@ -172,7 +177,7 @@ int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref, const double *
         DBuf<vqb::TableTask> dtasks(tasks.data(), tasks.size());
         vqb::launch_plane(dpj.p, 1, (int)nb, (int)width, e.stream());
         vqb::launch_ref_terms(dtj.p, (int)tj.size(), (int)nb, (int)patch, e.stream());
-        vqb::launch_table(dtasks.p, (int)tasks.size(), (int)nb, (int)patch, e.stream());
+        vqb::launch_table(dtasks.p, (int)tasks.size(), (int)nb, (int)patch, false, e.stream());
         VQB_CUDA(cudaStreamSynchronize(e.stream()));
         sims.get(out, np * nf_deg);
     });

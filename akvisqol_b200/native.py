@@ -90,6 +90,20 @@ class Timing(ctypes.Structure):
     ]
 
 
+class ServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", c_uint64), ("lanes", c_uint32), ("max_batch", c_uint32)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("queued", c_uint64),
+        ("in_flight", c_uint64), ("batches", c_uint64), ("hbm_budget_bytes", c_uint64),
+        ("hbm_in_flight_bytes", c_uint64), ("hbm_reserved_bytes", c_uint64),
+        ("latency_p50_ms", c_double), ("latency_p99_ms", c_double), ("latency_mean_ms", c_double),
+        ("queue_p50_ms", c_double), ("queue_p99_ms", c_double), ("mean_batch", c_double),
+    ]
+
+
 def build() -> Path:
     """Compile libvisqol.so with the package Makefile (no-op when current)."""
     subprocess.run(["make", "-s", "-j8", "-C", str(HERE)], check=True)
@@ -136,6 +150,13 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_dp_static": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
         "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
         "visqol_b200_peak": (c_int, [c_int, D]),
+        "visqol_b200_server_create": (c_int, [POINTER(Options), POINTER(ServeConfig), POINTER(c_void_p)]),
+        "visqol_b200_server_destroy": (None, [c_void_p]),
+        "visqol_b200_server_submit": (c_int, [c_void_p, c_uint32, c_void_p, c_size_t, c_void_p, c_size_t, c_uint32,
+                                              c_uint32, POINTER(c_uint64)]),
+        "visqol_b200_server_next": (c_int, [c_void_p, c_int32, POINTER(c_uint64), POINTER(c_int32),
+                                            POINTER(POINTER(Result))]),
+        "visqol_b200_server_stats": (c_int, [c_void_p, POINTER(ServeStats), c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -162,6 +183,8 @@ EXPORTS = [
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
+    "visqol_b200_server_create", "visqol_b200_server_destroy", "visqol_b200_server_submit",
+    "visqol_b200_server_next", "visqol_b200_server_stats",
 ]
 
 
@@ -457,3 +480,73 @@ def patch_similarity(ref, deg):
     _check(lib.visqol_b200_patch_similarity(_ptr(r), _ptr(d), nr, nc, _ptr(means), _ptr(sd), _ptr(en),
                                             ctypes.byref(mean)))
     return mean.value, means, sd, en
+
+
+PENDING = 1
+
+
+class Server:
+    """Owns a ``visqol_b200_server``: requests submitted one at a time from
+    any thread, scored in continuously refilled batches on the GPU."""
+
+    def __init__(self, *, precision: str = "exact", lanes: int = 0, max_batch: int = 0, hbm_budget_bytes: int = 0,
+                 search_window_radius: int = 60, disable_global_alignment: bool = False,
+                 disable_realignment: bool = False, use_unscaled_speech_mos_mapping: bool = False):
+        opts = Options()
+        lib.visqol_options_default(ctypes.byref(opts))
+        opts.precision = PRECISIONS[precision]
+        opts.search_window_radius = search_window_radius
+        opts.disable_global_alignment = int(bool(disable_global_alignment))
+        opts.disable_realignment = int(bool(disable_realignment))
+        opts.use_unscaled_speech_mos_mapping = int(bool(use_unscaled_speech_mos_mapping))
+        opts.use_lattice_model = 0
+        cfg = ServeConfig(hbm_budget_bytes, lanes, max_batch)
+        handle = c_void_p()
+        _check(lib.visqol_b200_server_create(ctypes.byref(opts), ctypes.byref(cfg), ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            lib.visqol_b200_server_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, mode: int, ref, deg, sample_rate: int, device_inputs: bool = False,
+               ref_len: int | None = None, deg_len: int | None = None) -> int:
+        """Queue one pair; host arrays are copied before this returns. With
+        device_inputs, ref/deg are device addresses (ints) that must stay
+        valid until the request completes."""
+        t = c_uint64()
+        if device_inputs:
+            rp, dp, rl, dl = c_void_p(ref), c_void_p(deg), ref_len, deg_len
+        else:
+            ref = np.ascontiguousarray(ref, dtype=np.float64)
+            deg = np.ascontiguousarray(deg, dtype=np.float64)
+            rp, dp, rl, dl = ref.ctypes.data_as(c_void_p), deg.ctypes.data_as(c_void_p), ref.size, deg.size
+        _check(lib.visqol_b200_server_submit(self._handle, mode, rp, rl, dp, dl, sample_rate,
+                                             DEVICE_INPUTS if device_inputs else 0, ctypes.byref(t)))
+        return t.value
+
+    def next(self, timeout_ms: int = -1):
+        """(ticket, status, result dict or None) of the next completed
+        request, or None when nothing completed within timeout_ms."""
+        t, st, out = c_uint64(), c_int32(), POINTER(Result)()
+        rc = lib.visqol_b200_server_next(self._handle, timeout_ms, ctypes.byref(t), ctypes.byref(st),
+                                         ctypes.byref(out))
+        if rc == PENDING:
+            return None
+        _check(rc)
+        res = None
+        if out:
+            try:
+                res = result_dict(out.contents)
+            finally:
+                lib.visqol_result_free(out)
+        return t.value, st.value, res
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServeStats()
+        _check(lib.visqol_b200_server_stats(self._handle, ctypes.byref(st), int(bool(reset))))
+        return {name: getattr(st, name) for name, _ in ServeStats._fields_}

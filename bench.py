@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fast", choices=["fast", "balanced", "exact"])
     p.add_argument("--only", action="store_true", help="time the --precision form alone")
+    p.add_argument("--serve-requests", type=int, default=5000,
+                   help="requests per offered load in the serving sweep (0: skip the sweep)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -192,6 +194,81 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SERVE_LOADS = (0.25, 0.5, 0.75, 1.0, 1.2)
+
+
+def serve_sweep(native, torch, precision: str, pool, n_req: int, seed: int) -> dict:
+    """Poisson arrivals of the serving mix (70% audio 48 kHz 2-60 s, 30%
+    speech 16 kHz 2-20 s) into a visqol_b200_server, signals resident in
+    HBM. Peak = pairs/s with every request queued at once; then each offered
+    load (a fraction of that peak) runs n_req requests and reports achieved
+    pairs/s and submit-to-result latency percentiles."""
+    import threading
+    rng = np.random.default_rng(seed)
+    dev = [(mode, sr, torch.from_numpy(p[0]).cuda(), torch.from_numpy(p[1]).cuda()) for mode, sr, p in pool]
+    audio = [i for i, d in enumerate(dev) if d[0] == 0]
+    speech = [i for i, d in enumerate(dev) if d[0] == 1]
+    torch.cuda.synchronize()
+
+    server = native.Server(precision=precision, lanes=4, max_batch=64)
+
+    def submit(i):
+        mode, sr, r, d = dev[i]
+        server.submit(mode, r.data_ptr(), d.data_ptr(), sr, device_inputs=True, ref_len=r.numel(), deg_len=d.numel())
+
+    # warm-up: every pool pair once (engines, rate caches, FFT tables, arenas)
+    for rep in range(2):
+        for i in range(len(dev)):
+            submit(i)
+        for _ in range(len(dev)):
+            server.next(timeout_ms=600000)
+    server.stats(reset=True)
+
+    def run(rate):
+        picks = [audio[rng.integers(len(audio))] if rng.random() < 0.7 else speech[rng.integers(len(speech))]
+                 for _ in range(n_req)]
+        gaps = rng.exponential(1.0 / rate, n_req) if rate else np.zeros(n_req)
+        failures = [0]
+
+        def produce():
+            t_next = time.perf_counter()
+            for k, i in enumerate(picks):
+                t_next += gaps[k]
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                submit(i)
+
+        t0 = time.perf_counter()
+        th = threading.Thread(target=produce)
+        th.start()
+        for _ in range(n_req):
+            item = server.next(timeout_ms=600000)
+            if item is None or item[1] != 0:
+                failures[0] += 1
+        wall = time.perf_counter() - t0
+        th.join()
+        st = server.stats(reset=True)
+        return {"offered_pairs_per_s": rate, "pairs_per_s": n_req / wall, "latency_p50_ms": st["latency_p50_ms"],
+                "latency_p99_ms": st["latency_p99_ms"], "queue_p99_ms": st["queue_p99_ms"],
+                "mean_batch": st["mean_batch"], "failures": failures[0]}
+
+    peak = run(None)["pairs_per_s"]
+    loads = [dict(load=f, **run(f * peak)) for f in SERVE_LOADS]
+    server.close()
+    return {"requests_per_load": n_req, "peak_pairs_per_s": peak, "loads": loads,
+            "mix": "70% audio 48 kHz log-uniform 2-60 s, 30% speech 16 kHz log-uniform 2-20 s; "
+                   f"{len(pool)} distinct seeded pairs resident in HBM, drawn per request",
+            "lanes": 4, "max_batch": 64}
+
+
+def serve_pool(seed0: int, n_audio: int = 70, n_speech: int = 30):
+    from akvisqol_b200 import synth
+    pool = [(0, 48000, p) for p in synth.audio_batch(n_audio, seed0=seed0, min_s=2.0, max_s=60.0)]
+    pool += [(1, 16000, p) for p in synth.speech_batch(n_speech, seed0=seed0 + 0x8000, min_s=2.0, max_s=20.0)]
+    return pool
+
+
 def run_ours(args, rank, world, local):
     os.environ["VISQOL_CUDA_DEVICE"] = str(local)
     import torch
@@ -265,7 +342,7 @@ def run_ours(args, rank, world, local):
     for _ in range(args.steps):
         t0 = time.perf_counter()
         outs = ctx.measure_batch(pin_r, pin_d, 48000)
-        moses = [native.result_dict(o.contents)["moslqo"] for o in outs if not isinstance(o, native.NativeError)]
+        moses = [o.contents.moslqo for o in outs if not isinstance(o, native.NativeError)]
         for o in outs:
             if not isinstance(o, native.NativeError):
                 native.free(o)
@@ -319,6 +396,11 @@ def run_ours(args, rank, world, local):
         "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline": r["roofline"],
                       "failures": r["failures"]} for f, r in runs.items()},
     }
+    if args.serve_requests > 0:
+        pool = serve_pool(0x5EED_4000 + 7919 * rank)
+        line["serving"] = {f: serve_sweep(native, torch, f, pool, args.serve_requests, 17 + rank)
+                           for f in dict.fromkeys([args.precision, "exact"])}
+        del pool
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(pairs, args.seconds)
         res = cb.pop("results")

@@ -75,6 +75,63 @@ int visqol_b200_measure_batch(visqol_ctx *ctx, size_t n,
 void visqol_b200_trace_free(visqol_b200_trace *trace);
 int visqol_b200_last_timing(visqol_ctx *ctx, visqol_b200_timing *out);
 
+/* ---- request server: continuous batching on one GPU ---------------------
+ * No counterpart in the reference (its batch call is synchronous). Requests
+ * are submitted one at a time from any thread and complete asynchronously.
+ * A pool of lanes (engines with their own streams) runs on the GPU at once;
+ * a lane that finishes a batch immediately takes the requests queued
+ * meanwhile (oldest first, one mode and sample rate per batch) up to
+ * max_batch pairs and its share of the HBM budget, estimated per pair from
+ * the signal lengths. So requests that arrive while others are on the GPU
+ * are admitted as lanes and memory free up, and their work overlaps the
+ * other lanes' work on the device. Results do not depend on which requests
+ * share a batch. */
+typedef struct visqol_b200_server visqol_b200_server;
+
+typedef struct {
+    uint64_t hbm_budget_bytes; /* device memory for in-flight pairs; 0: half of the free memory */
+    uint32_t lanes;            /* concurrent batches; 0: 4 */
+    uint32_t max_batch;        /* pairs per batch; 0: 64 */
+} visqol_b200_serve_config;
+
+typedef struct {
+    uint64_t submitted, completed, failed, queued, in_flight;
+    uint64_t batches;               /* batches run */
+    uint64_t hbm_budget_bytes;      /* admission budget (all lanes) */
+    uint64_t hbm_in_flight_bytes;   /* estimated footprint of the pairs on the GPU now */
+    uint64_t hbm_reserved_bytes;    /* device memory the lanes hold */
+    double latency_p50_ms, latency_p99_ms, latency_mean_ms; /* submit -> result, completed since reset */
+    double queue_p50_ms, queue_p99_ms;                     /* submit -> admitted */
+    double mean_batch;              /* pairs per batch */
+} visqol_b200_serve_stats;
+
+/* Server for the options' precision, radius and flags; `mode` of opts is
+ * ignored (each request names its own). Speech requests need
+ * use_lattice_model = 0. */
+int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serve_config *cfg,
+                              visqol_b200_server **out);
+/* Stops taking requests, finishes those admitted, frees everything (results
+ * not yet collected are freed too). */
+void visqol_b200_server_destroy(visqol_b200_server *s);
+/* Queue one pair (mode VISQOL_MODE_AUDIO or _SPEECH). Host signals are
+ * copied before the call returns; with VISQOL_B200_DEVICE_INPUTS the device
+ * pointers must stay valid until the request completes. A pair whose
+ * estimated footprint exceeds one lane's share of the budget fails with
+ * VISQOL_E_OUT_OF_MEMORY. */
+int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double *ref, size_t ref_len,
+                              const double *deg, size_t deg_len, uint32_t sample_rate, uint32_t flags,
+                              uint64_t *ticket);
+/* Next completed request in completion order, waiting up to timeout_ms
+ * (< 0: no limit). Returns VISQOL_OK with *ticket, *status (the pair's
+ * code) and *out (NULL on failure; free with visqol_result_free), or
+ * VISQOL_B200_PENDING when nothing completed in time. */
+#define VISQOL_B200_PENDING 1
+int visqol_b200_server_next(visqol_b200_server *s, int32_t timeout_ms, uint64_t *ticket, int32_t *status,
+                            visqol_result **out);
+/* Counters and latency percentiles; reset != 0 clears the latency samples
+ * and the batch counters after reading. */
+int visqol_b200_server_stats(visqol_b200_server *s, visqol_b200_serve_stats *out, int reset);
+
 /* Device name, SM count and compute capability of the context's GPU. */
 int visqol_b200_device_info(int device, char *name, size_t name_len,
                             int *sm_count, int *cc_major, int *cc_minor);

@@ -63,6 +63,27 @@ def test_no_device_refuses_without_fallback(native):
     assert e.value.code == native.E_BACKEND
 
 
+@pytest.mark.skipif(bool(os.environ.get("CUDA_VISIBLE_DEVICES_FORCE")), reason="forced device")
+def test_server_needs_a_device(native):
+    if native.available_backends():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(native.NativeError) as e:
+        native.Server(precision="fast")
+    assert e.value.code == native.E_BACKEND
+
+
+def test_server_argument_errors(native):
+    o = native.Options()
+    native.lib.visqol_options_default(ctypes.byref(o))
+    o.backend = 0
+    h = ctypes.c_void_p()
+    assert native.lib.visqol_b200_server_create(ctypes.byref(o), None, ctypes.byref(h)) == native.E_BACKEND
+    assert native.lib.visqol_b200_server_create(None, None, None) == native.E_INVALID_ARGUMENT
+    t = ctypes.c_uint64()
+    assert native.lib.visqol_b200_server_submit(None, 0, None, 0, None, 0, 48000, 0, ctypes.byref(t)) == \
+        native.E_INVALID_ARGUMENT
+
+
 def test_speech_lattice_is_reported(native):
     with pytest.raises(native.NativeError) as e:
         native.Context(mode=native.MODE_SPEECH, use_lattice_model=True)
