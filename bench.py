@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--only", action="store_true", help="time the --precision form alone")
     p.add_argument("--serve-requests", type=int, default=5000,
                    help="requests per offered load in the serving sweep (0: skip the sweep)")
+    p.add_argument("--config-pairs", type=int, default=256,
+                   help="pairs per mode in the uneven-batch accuracy and throughput runs (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -197,6 +199,62 @@ def run_reference(args, rank, world):
 SERVE_LOADS = (0.25, 0.5, 0.75, 1.0, 1.2)
 
 
+def uneven_configs(native, torch, n: int, plain_exact: float) -> dict:
+    """The uneven batches: n audio pairs (48 kHz, log-uniform 3-30 s, cutoff
+    4-16 kHz, SNR 10-40 dB, delay 0-200 ms) and n speech pairs (16 kHz,
+    2-15 s). Batched pairs/s per form (signals in HBM, one batch per mode),
+    and per form the per-pair |dMOS| against the CPU model with agreement of
+    global lags, patch indices (VAD in speech mode) and matched offsets."""
+    import oracle
+    from akvisqol_b200 import synth
+    sets = {"audio": (native.MODE_AUDIO, 48000, synth.audio_batch(n, min_s=3.0, max_s=30.0)),
+            "speech": (native.MODE_SPEECH, 16000, synth.speech_batch(n, min_s=2.0, max_s=15.0))}
+    threads = os.cpu_count() or 1
+    out = {}
+    for name, (mode, sr, pairs) in sets.items():
+        refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
+        t0 = time.perf_counter()
+        res = oracle.measure_batch(refs, degs, sr, oracle.options(mode=mode), threads=threads)
+        cpu_s = time.perf_counter() - t0
+        d_ref = [torch.from_numpy(r).cuda() for r in refs]
+        d_deg = [torch.from_numpy(d).cuda() for d in degs]
+        torch.cuda.synchronize()
+        entry = {"pairs": n, "seconds_total": float(sum(r.size for r in refs)) / sr,
+                 "cpu_model_pairs_per_s": n / cpu_s, "cpu_threads": threads}
+        for form in ("exact", "balanced", "fast"):
+            ctx = native.Context(mode=mode, use_lattice_model=False, precision=form)
+            args = ([t.data_ptr() for t in d_ref], [t.data_ptr() for t in d_deg], sr)
+            kw = dict(device_inputs=True, ref_lens=[t.numel() for t in d_ref], deg_lens=[t.numel() for t in d_deg])
+            ctx.measure_batch_traced(*args, **kw)  # warm
+            got = ctx.measure_batch_traced(*args, **kw)
+            ms = ctx.last_timing()["total_ms"]
+            dm = [abs(g[1]["moslqo"] - w[1]["moslqo"]) for g, w in zip(got, res) if g[0] == 0 and w[0] == 0]
+            entry[form] = {"pairs_per_s": n / (ms / 1e3), "failures": sum(1 for g in got if g[0] != 0),
+                           "max_abs_dmos": max(dm) if dm else None,
+                           "p99_abs_dmos": float(np.percentile(dm, 99)) if dm else None,
+                           "median_abs_dmos": float(np.median(dm)) if dm else None,
+                           "pairs_over_1e-6": int(sum(1 for v in dm if v > 1e-6))}
+            del ctx
+        entry["exact_speedup_vs_plain_exact"] = entry["exact"]["pairs_per_s"] / plain_exact if mode == 0 else None
+        # discrete decisions of every form against the CPU model on a subset (traces are per pair)
+        k = min(n, 24)
+        wtrs = [oracle.measure(r, d, sr, oracle.options(mode=mode))[1] for r, d in zip(refs[:k], degs[:k])]
+        agree = {f: 0 for f in ("exact", "balanced", "fast")}
+        for form in agree:
+            ctx = native.Context(mode=mode, use_lattice_model=False, precision=form)
+            got = ctx.measure_batch_traced(refs[:k], degs[:k], sr)
+            for (c, _, tr), wtr in zip(got, wtrs):
+                agree[form] += int(c == 0 and tr["global_lag"] == wtr["global_lag"]
+                                   and list(tr["ref_index"]) == list(wtr["ref_index"])
+                                   and list(tr["deg_offset"]) == list(wtr["deg_offset"])
+                                   and list(tr["realign_lag"]) == list(wtr["realign_lag"]))
+            del ctx
+        entry["decisions_identical"] = {f: f"{v}/{k}" for f, v in agree.items()}
+        out[name] = entry
+        del d_ref, d_deg
+    return out
+
+
 def serve_sweep(native, torch, precision: str, pool, n_req: int, seed: int) -> dict:
     """Poisson arrivals of the serving mix (70% audio 48 kHz 2-60 s, 30%
     speech 16 kHz 2-20 s) into a visqol_b200_server, signals resident in
@@ -253,10 +311,29 @@ def serve_sweep(native, torch, precision: str, pool, n_req: int, seed: int) -> d
                 "latency_p99_ms": st["latency_p99_ms"], "queue_p99_ms": st["queue_p99_ms"],
                 "mean_batch": st["mean_batch"], "failures": failures[0]}
 
-    peak = run(None)["pairs_per_s"]
+    def saturate(window: int):
+        """Closed loop: keep `window` requests outstanding; sustained pairs/s."""
+        picks = [audio[rng.integers(len(audio))] if rng.random() < 0.7 else speech[rng.integers(len(speech))]
+                 for _ in range(n_req)]
+        t0 = time.perf_counter()
+        sent = 0
+        for _ in range(min(window, n_req)):
+            submit(picks[sent])
+            sent += 1
+        for _ in range(n_req):
+            server.next(timeout_ms=600000)
+            if sent < n_req:
+                submit(picks[sent])
+                sent += 1
+        wall = time.perf_counter() - t0
+        server.stats(reset=True)
+        return n_req / wall
+
+    peak = saturate(4 * 64)
     loads = [dict(load=f, **run(f * peak)) for f in SERVE_LOADS]
     server.close()
-    return {"requests_per_load": n_req, "peak_pairs_per_s": peak, "loads": loads,
+    return {"requests_per_load": n_req, "peak_pairs_per_s": peak,
+            "peak_definition": "closed loop with lanes x max_batch = 256 requests outstanding", "loads": loads,
             "mix": "70% audio 48 kHz log-uniform 2-60 s, 30% speech 16 kHz log-uniform 2-20 s; "
                    f"{len(pool)} distinct seeded pairs resident in HBM, drawn per request",
             "lanes": 4, "max_batch": 64}
@@ -396,6 +473,8 @@ def run_ours(args, rank, world, local):
         "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline": r["roofline"],
                       "failures": r["failures"]} for f, r in runs.items()},
     }
+    if args.config_pairs > 0 and rank == 0:
+        line["uneven_batches"] = uneven_configs(native, torch, args.config_pairs, plain_value)
     if args.serve_requests > 0:
         pool = serve_pool(0x5EED_4000 + 7919 * rank)
         line["serving"] = {f: serve_sweep(native, torch, f, pool, args.serve_requests, 17 + rank)
