@@ -31,6 +31,14 @@ using vqb::Error;
 // GPU engine, src/gpu/engine.zig:551-591). A batch is split across the
 // lanes by signal length and the lanes run concurrently from host threads,
 // so one lane's serial phases and host planning overlap another's kernels.
+// References prepared once for many degraded signals (visqol_b200_prepare).
+struct visqol_b200_prepared {
+    int device = 0;
+    vqb::Options opt;
+    uint32_t sample_rate = 0;
+    std::vector<std::unique_ptr<vqb::PreparedRef>> refs;
+};
+
 struct visqol_ctx {
     vqb::Options opt;
     std::shared_ptr<const vqb::host::Svr> svr;
@@ -133,11 +141,12 @@ int device_count() {
 // The batch across the context's lanes: pairs dealt longest-first to the
 // least-loaded lane, lanes run concurrently, outcomes gathered back in order.
 void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
-               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, std::vector<vqb::PairOutcome> &res) {
+               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, std::vector<vqb::PairOutcome> &res,
+               const vqb::PreparedRef *const *prepared = nullptr) {
     const size_t L = std::min(c->lanes.size(), std::max<size_t>(1, n));
     res.assign(n, vqb::PairOutcome{});
     if (L <= 1) {
-        c->lanes[0]->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
+        c->lanes[0]->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res, prepared);
         c->timing = c->lanes[0]->last_timing();
         return;
     }
@@ -160,10 +169,13 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
             const auto &ix = part[l];
             std::vector<const double *> r(ix.size()), d(ix.size());
             std::vector<size_t> rl(ix.size()), dl(ix.size());
-            for (size_t k = 0; k < ix.size(); ++k)
+            std::vector<const vqb::PreparedRef *> pr(prepared ? ix.size() : 0);
+            for (size_t k = 0; k < ix.size(); ++k) {
                 r[k] = refs[ix[k]], d[k] = degs[ix[k]], rl[k] = ref_lens[ix[k]], dl[k] = deg_lens[ix[k]];
+                if (prepared) pr[k] = prepared[ix[k]];
+            }
             c->lanes[l]->measure_batch(ix.size(), r.data(), rl.data(), d.data(), dl.data(), sample_rate, device_inputs,
-                                       lane_out[l]);
+                                       lane_out[l], prepared ? pr.data() : nullptr);
         } catch (...) {
             errs[l] = std::current_exception();
         }
@@ -200,10 +212,10 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
 // One batch through the engine with per-pair results and status.
 int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, visqol_result **out, int32_t *status,
-              visqol_b200_trace **traces) {
+              visqol_b200_trace **traces, const vqb::PreparedRef *const *prepared = nullptr) {
     std::vector<vqb::PairOutcome> res;
     try {
-        run_lanes(c, n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res);
+        run_lanes(c, n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res, prepared);
     } catch (const Error &e) {
         for (size_t i = 0; i < n; ++i) {
             out[i] = nullptr;
@@ -472,6 +484,53 @@ int visqol_b200_measure_batch(visqol_ctx *c, size_t n, const double *const *refs
     if (!out || !refs || !ref_lens || !degs || !deg_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
     return run_batch(c, n, refs, ref_lens, degs, deg_lens, sample_rate, (flags & VISQOL_B200_DEVICE_INPUTS) != 0, out,
                      status, traces);
+}
+
+int visqol_b200_prepare(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,
+                        uint32_t sample_rate, uint32_t flags, visqol_b200_prepared **out) {
+    if (!c || !out) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (n && (!refs || !ref_lens)) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    if (sample_rate == 0) return fail(VISQOL_E_INVALID_ARGUMENT, "sample_rate is 0");
+    try {
+        auto p = std::make_unique<visqol_b200_prepared>();
+        p->device = c->lanes[0]->device();
+        p->opt = c->opt;
+        p->sample_rate = sample_rate;
+        c->lanes[0]->prepare(n, refs, ref_lens, sample_rate, (flags & VISQOL_B200_DEVICE_INPUTS) != 0, p->refs);
+        *out = p.release();
+        return VISQOL_OK;
+    } catch (const Error &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(VISQOL_E_OUT_OF_MEMORY, "OutOfMemory");
+    } catch (const std::exception &e) {
+        return fail(VISQOL_E_INTERNAL, e.what());
+    }
+}
+
+void visqol_b200_prepared_free(visqol_b200_prepared *p) { delete p; }
+
+int visqol_b200_measure_prepared(visqol_ctx *c, const visqol_b200_prepared *p, size_t n, const size_t *ref_index,
+                                 const double *const *degs, const size_t *deg_lens, uint32_t flags,
+                                 visqol_result **out, int32_t *status) {
+    if (!c || !p) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return VISQOL_OK;
+    if (!out || !degs || !deg_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    if (p->device != c->lanes[0]->device() || p->opt.form != c->opt.form || p->opt.speech != c->opt.speech)
+        return fail(VISQOL_E_INVALID_ARGUMENT, "prepared references come from a context of another device, "
+                                               "mode or precision");
+    std::vector<const vqb::PreparedRef *> prep(n);
+    std::vector<const double *> rp(n, nullptr);
+    std::vector<size_t> rl(n);
+    for (size_t i = 0; i < n; ++i) {
+        const size_t k = ref_index ? ref_index[i] : i;
+        if (k >= p->refs.size()) return fail(VISQOL_E_INVALID_ARGUMENT, "ref_index out of range");
+        prep[i] = p->refs[k].get();
+        rl[i] = prep[i]->len;
+    }
+    return run_batch(c, n, rp.data(), rl.data(), degs, deg_lens, p->sample_rate,
+                     (flags & VISQOL_B200_DEVICE_INPUTS) != 0, out, status, nullptr, prep.data());
 }
 
 void visqol_b200_trace_free(visqol_b200_trace *t) {

@@ -291,6 +291,115 @@ size_t Engine::pair_footprint(size_t rl, size_t dl, uint32_t sample_rate, bool s
     return b;
 }
 
+uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const RateCache &rc, cudaStream_t st,
+                                     cudaEvent_t begin, cudaEvent_t end) {
+    if (jobs.empty()) return 0;
+    const int nbi = (int)nb_;
+    const int W = (int)rc.geo.window, H = (int)rc.geo.hop;
+    SpecJob *d_jobs = upload(jobs);
+    const int F = opt_.form == kFormF32 ? gammatone_fast_frames_per_cta() : gammatone_frames_per_cta(nbi);
+    const size_t tsz = gammatone_tile_size();
+    std::vector<char> tiles;
+    int ntiles = 0;
+    uint64_t rms = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        rms += (uint64_t)jobs[j].nf * nb_;
+        for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
+            tiles.resize(tiles.size() + tsz);
+            fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+        }
+    }
+    void *d_tiles = upload_bytes(tiles.data(), tiles.size());
+    if (st != stream_) {
+        // job tables were copied on the main stream
+        record(ev_inputs_);
+        VQB_CUDA(cudaStreamWaitEvent(st, ev_inputs_, 0));
+    }
+    if (begin) VQB_CUDA(cudaEventRecord(begin, st));
+    if (opt_.form == kFormF32)
+        launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
+    else if (opt_.form == kFormF64)
+        launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
+    else
+        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, W, H, st);
+    if (end) VQB_CUDA(cudaEventRecord(end, st));
+    return rms;
+}
+
+PreparedRef::~PreparedRef() {
+    if (!d_sig && !d_stats && !d_spec) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    cudaFree(d_sig);
+    cudaFree(d_stats);
+    cudaFree(d_spec);
+    cudaSetDevice(cur);
+}
+
+void Engine::prepare(size_t n, const double *const *refs, const size_t *ref_lens, uint32_t sample_rate,
+                     bool device_inputs, std::vector<std::unique_ptr<PreparedRef>> &out) {
+    out.clear();
+    VQB_CUDA(cudaSetDevice(device_));
+    arena_.reset();
+    pinned_.reset();
+    const RateCache &rc = rate_cache(sample_rate);
+    const size_t W = rc.geo.window, H = rc.geo.hop, P = patch_;
+    std::vector<SumJob> sums;
+    std::vector<SpecJob> specs;
+    for (size_t i = 0; i < n; ++i) {
+        auto p = std::make_unique<PreparedRef>();
+        p->device = device_;
+        p->len = ref_lens[i];
+        if (p->len && !refs[i]) {
+            p->code = kInvalid;
+            p->message = "signal pointer is NULL";
+        } else if (p->len <= W) {
+            p->code = kSignal;
+            p->message = "SpectrogramTooShort";
+        } else {
+            p->nf = host::num_frames(p->len, W, H);
+            VQB_CUDA(cudaMalloc(&p->d_sig, p->len * sizeof(double)));
+            VQB_CUDA(cudaMalloc(&p->d_stats, 4 * sizeof(double)));
+            VQB_CUDA(cudaMalloc(&p->d_spec, nb_ * p->nf * sizeof(double)));
+            VQB_CUDA(cudaMemcpyAsync(p->d_sig, refs[i], p->len * sizeof(double),
+                                     device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+            const VSig sig{p->d_sig, 0, (int64_t)p->len, (int64_t)p->len};
+            sums.push_back(SumJob{sig, p->d_stats});
+            specs.push_back(SpecJob{sig, (int64_t)p->nf, p->d_spec});
+        }
+        out.push_back(std::move(p));
+    }
+    launch_sums(sums);
+    launch_spectrograms(specs, rc, stream_);
+    std::vector<double> h(4 * n, 0.0);
+    for (size_t i = 0; i < n; ++i)
+        if (out[i]->d_stats) VQB_CUDA(cudaMemcpyAsync(h.data() + 4 * i, out[i]->d_stats, 4 * sizeof(double),
+                                                      cudaMemcpyDeviceToHost, stream_));
+    sync();
+    for (size_t i = 0; i < n; ++i) {
+        PreparedRef &p = *out[i];
+        if (p.code) continue;
+        std::copy(h.begin() + 4 * i, h.begin() + 4 * i + 4, p.stats);
+        if (opt_.speech) {
+            std::vector<double> tmp;
+            const double *hr = refs[i];
+            if (device_inputs) {
+                tmp.resize(p.len);
+                VQB_CUDA(cudaMemcpy(tmp.data(), refs[i], p.len * sizeof(double), cudaMemcpyDeviceToHost));
+                hr = tmp.data();
+            }
+            p.idx = host::vad_patch_indices(hr, p.len, p.nf, P, W, 0.25);
+        } else {
+            p.idx = host::ref_patch_indices(p.nf, P);
+        }
+        if (p.idx.empty()) {
+            p.code = kSignal;
+            p.message = "NoPatches";
+        }
+    }
+}
+
 void Engine::launch_sums(const std::vector<SumJob> &sums) {
     if (sums.empty()) return;
     const SumJob *d = upload(sums);
@@ -370,6 +479,7 @@ struct RealignPatch {
 };
 
 struct PairState {
+    const PreparedRef *prep = nullptr;
     bool live = true;
     int code = 0;
     std::string msg;
@@ -404,7 +514,7 @@ struct PairState {
 
 void Engine::measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                            const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
-                           std::vector<PairOutcome> &out) {
+                           std::vector<PairOutcome> &out, const PreparedRef *const *prepared) {
     out.assign(n, PairOutcome{});
     timing_ = Timing{};
     if (n == 0) return;
@@ -426,57 +536,43 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     // ---- inputs -----------------------------------------------------------
     for (size_t i = 0; i < n; ++i) {
         PairState &s = ps[i];
-        s.rl = ref_lens[i];
+        s.prep = prepared ? prepared[i] : nullptr;
+        if (s.prep && s.prep->code) {
+            s.fail(s.prep->code, s.prep->message);
+            continue;
+        }
+        s.rl = s.prep ? s.prep->len : ref_lens[i];
         s.dl = deg_lens[i];
-        if ((s.rl && !refs[i]) || (s.dl && !degs[i])) {
+        if ((!s.prep && s.rl && !refs[i]) || (s.dl && !degs[i])) {
             s.fail(kInvalid, "signal pointer is NULL");
             continue;
         }
         if (device_inputs) {
-            s.ref = refs[i];
+            s.ref = s.prep ? s.prep->d_sig : refs[i];
             s.deg = degs[i];
         } else {
-            double *r = arena_.alloc_n<double>(s.rl), *d = arena_.alloc_n<double>(s.dl);
-            if (s.rl) VQB_CUDA(cudaMemcpyAsync(r, refs[i], s.rl * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            double *d = arena_.alloc_n<double>(s.dl);
             if (s.dl) VQB_CUDA(cudaMemcpyAsync(d, degs[i], s.dl * sizeof(double), cudaMemcpyHostToDevice, stream_));
-            timing_.h2d_bytes += (s.rl + s.dl) * sizeof(double);
-            s.ref = r;
+            timing_.h2d_bytes += s.dl * sizeof(double);
             s.deg = d;
-            s.h_ref = refs[i];
+            if (s.prep) {
+                s.ref = s.prep->d_sig;
+            } else {
+                double *r = arena_.alloc_n<double>(s.rl);
+                if (s.rl)
+                    VQB_CUDA(cudaMemcpyAsync(r, refs[i], s.rl * sizeof(double), cudaMemcpyHostToDevice, stream_));
+                timing_.h2d_bytes += s.rl * sizeof(double);
+                s.ref = r;
+                s.h_ref = refs[i];
+            }
         }
         s.stats = arena_.alloc_n<double>(10);
     }
 
     auto run_gammatone = [&](const std::vector<SpecJob> &jobs, cudaStream_t st) {
         if (jobs.empty()) return;
-        SpecJob *d_jobs = upload(jobs);
-        const int F = opt_.form == kFormF32 ? gammatone_fast_frames_per_cta() : gammatone_frames_per_cta(nbi);
-        const size_t tsz = gammatone_tile_size();
-        std::vector<char> tiles;
-        int ntiles = 0;
-        uint64_t rms = 0;
-        for (size_t j = 0; j < jobs.size(); ++j) {
-            rms += (uint64_t)jobs[j].nf * NB;
-            for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
-                tiles.resize(tiles.size() + tsz);
-                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
-            }
-        }
-        void *d_tiles = upload_bytes(tiles.data(), tiles.size());
-        if (st != stream_) {
-            // job tables were copied on the main stream
-            record(ev_inputs_);
-            VQB_CUDA(cudaStreamWaitEvent(st, ev_inputs_, 0));
-        }
         const size_t slot = 2 * timing_.gammatone_launches;
-        VQB_CUDA(cudaEventRecord(gt_events_[slot], st));
-        if (opt_.form == kFormF32)
-            launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
-        else if (opt_.form == kFormF64)
-            launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
-        else
-            launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, (int)W, (int)H, st);
-        VQB_CUDA(cudaEventRecord(gt_events_[slot + 1], st));
+        const uint64_t rms = launch_spectrograms(jobs, rc, st, gt_events_[slot], gt_events_[slot + 1]);
         timing_.gammatone_launches += 1;
         timing_.gammatone_rms += rms;
         timing_.gammatone_window = W;
@@ -489,6 +585,11 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         for (size_t i = 0; i < n; ++i) {
             PairState &s = ps[i];
             if (!s.live || s.rl <= W) continue;
+            if (s.prep) {
+                s.nf_ref = s.prep->nf;
+                s.ref_raw = s.prep->d_spec;
+                continue;
+            }
             s.nf_ref = host::num_frames(s.rl, W, H);
             s.ref_raw = arena_.alloc_n<double>(NB * s.nf_ref);
             ref_jobs.push_back(SpecJob{VSig{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, (int64_t)s.nf_ref, s.ref_raw});
@@ -507,7 +608,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
             PairState &s = ps[i];
             if (!s.live) continue;
             const VSig r{s.ref, 0, (int64_t)s.rl, (int64_t)s.rl}, d{s.deg, 0, (int64_t)s.dl, (int64_t)s.dl};
-            sums.push_back(SumJob{r, s.stats});
+            if (!s.prep) sums.push_back(SumJob{r, s.stats});
             if (!opt_.disable_global_alignment && s.rl > 0 && s.dl > 0) {
                 s.lag_job = true;
                 sums.push_back(SumJob{d, s.stats + 4});
@@ -516,7 +617,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                 j.b = d;
                 j.biggest = (int64_t)std::max(s.rl, s.dl);
                 j.n = (int64_t)host::fft_size_for((size_t)j.biggest);
-                j.stats_a = s.stats;
+                j.stats_a = s.prep ? s.prep->d_stats : s.stats;
                 j.stats_b = s.stats + 4;
                 j.lag_out = d_lags + i;
                 lag_jobs.push_back(j);
@@ -549,6 +650,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         if (ps[i].live) d2h(h_stats + 10 * i, ps[i].stats, 10 * sizeof(double));
     record(events_[1]);
     sync();
+    for (size_t i = 0; i < n; ++i)
+        if (ps[i].live && ps[i].prep) std::copy(ps[i].prep->stats, ps[i].prep->stats + 4, h_stats + 10 * i);
 
     // ---- 2: plan frames, patches and search windows (host) --------------
     std::vector<SpecJob> spec_jobs;
@@ -580,7 +683,9 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
             s.nf_deg = host::num_frames((size_t)s.al.len, W, H);
             s.trace.nf_ref = s.nf_ref;
             s.trace.nf_deg = s.nf_deg;
-            if (opt_.speech) {
+            if (s.prep) {
+                s.idx = s.prep->idx;
+            } else if (opt_.speech) {
                 std::vector<double> tmp;
                 const double *hr = s.h_ref;
                 if (!hr) {

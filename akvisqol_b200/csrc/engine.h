@@ -91,6 +91,23 @@ private:
     size_t current_ = 0;
 };
 
+// A reference scored against many degraded signals: the work that depends
+// only on it, done once (reference src/visqol.zig:194-244, the prepared
+// references of src/gpu/pipeline.zig:336-472): its samples, envelope
+// statistics and raw spectrogram on the device, its patch indices (VAD in
+// speech mode) on the host. Computed by Engine::prepare in the engine's
+// form; device buffers are owned here.
+struct PreparedRef {
+    int code = 0;  // non-zero: the reference itself cannot be scored
+    std::string message;
+    int device = 0;
+    size_t len = 0, nf = 0;
+    double *d_sig = nullptr, *d_stats = nullptr, *d_spec = nullptr;
+    double stats[4] = {};  // host copy of d_stats: sum, nyquist term, energy, -
+    std::vector<int64_t> idx;
+    ~PreparedRef();
+};
+
 class Engine {
 public:
     Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr);
@@ -100,9 +117,15 @@ public:
 
     // Score n pairs at one sample rate. Pointers are host memory unless
     // device_inputs. Per-pair failures land in out[i].code.
+    // With prepared non-NULL, pair i whose prepared[i] is set takes its
+    // reference from there (refs[i] and ref_lens[i] are ignored).
     void measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                        const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
-                       std::vector<PairOutcome> &out);
+                       std::vector<PairOutcome> &out, const PreparedRef *const *prepared = nullptr);
+    // Reference-side work of n references in this engine's form and mode.
+    void prepare(size_t n, const double *const *refs, const size_t *ref_lens, uint32_t sample_rate,
+                 bool device_inputs, std::vector<std::unique_ptr<PreparedRef>> &out);
+    const Options &options() const { return opt_; }
 
     const Timing &last_timing() const { return timing_; }
     // Upper bound on the device memory one pair of these lengths takes in
@@ -134,6 +157,10 @@ private:
     };
     // Envelope statistics of sum jobs: serial (exact) or tree (fast).
     void launch_sums(const std::vector<SumJob> &sums);
+    // Gammatone spectrograms of the jobs in this engine's form on stream st;
+    // returns the RMS count.
+    uint64_t launch_spectrograms(const std::vector<SpecJob> &jobs, const RateCache &rc, cudaStream_t st,
+                                 cudaEvent_t begin = nullptr, cudaEvent_t end = nullptr);
     const RateCache &rate_cache(uint32_t sample_rate);
 
     // Envelope (or raw) lag search for jobs whose a/b/stat pointers are set;

@@ -150,6 +150,11 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_dp_static": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
         "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
         "visqol_b200_peak": (c_int, [c_int, D]),
+        "visqol_b200_prepare": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, c_uint32, c_uint32,
+                                        POINTER(c_void_p)]),
+        "visqol_b200_measure_prepared": (c_int, [c_void_p, c_void_p, c_size_t, SZ, POINTER(c_void_p), SZ, c_uint32,
+                                                 POINTER(POINTER(Result)), POINTER(c_int32)]),
+        "visqol_b200_prepared_free": (None, [c_void_p]),
         "visqol_b200_server_create": (c_int, [POINTER(Options), POINTER(ServeConfig), POINTER(c_void_p)]),
         "visqol_b200_server_destroy": (None, [c_void_p]),
         "visqol_b200_server_submit": (c_int, [c_void_p, c_uint32, c_void_p, c_size_t, c_void_p, c_size_t, c_uint32,
@@ -183,6 +188,7 @@ EXPORTS = [
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
+    "visqol_b200_prepare", "visqol_b200_measure_prepared", "visqol_b200_prepared_free",
     "visqol_b200_server_create", "visqol_b200_server_destroy", "visqol_b200_server_submit",
     "visqol_b200_server_next", "visqol_b200_server_stats",
 ]
@@ -280,6 +286,32 @@ class Context:
         status = (c_int32 * n)()
         lib.visqol_measure_batch(self._handle, n, ref_ptrs, ref_lens, deg_ptrs, deg_lens, sample_rate, num_threads,
                                  outs, status)
+        return _collect(outs, status, n)
+
+    def prepare(self, refs, sample_rate: int, device_inputs: bool = False, ref_lens=None) -> "Prepared":
+        """Reference-side work for scoring many degraded signals against
+        these references (visqol_b200_prepare)."""
+        return Prepared(self, refs, sample_rate, device_inputs, ref_lens)
+
+    def measure_prepared(self, prepared: "Prepared", degs, ref_index=None, device_inputs: bool = False,
+                         deg_lens=None):
+        """degs[i] against prepared reference ref_index[i] (default i):
+        per-pair Result pointers or NativeError, as measure_batch."""
+        n = len(degs)
+        if device_inputs:
+            dp = (c_void_p * n)(*degs)
+            dl = (c_size_t * n)(*deg_lens)
+        else:
+            degs = [np.ascontiguousarray(d, dtype=np.float64) for d in degs]
+            dp = (c_void_p * n)(*[d.ctypes.data for d in degs])
+            dl = (c_size_t * n)(*[d.size for d in degs])
+        ix = (c_size_t * n)(*ref_index) if ref_index is not None else None
+        outs = (POINTER(Result) * n)()
+        status = (c_int32 * n)()
+        rc = lib.visqol_b200_measure_prepared(self._handle, prepared._handle, n, ix, dp, dl,
+                                              DEVICE_INPUTS if device_inputs else 0, outs, status)
+        if rc != OK and all(status[i] == OK for i in range(n)):
+            raise last_error(rc)  # the call itself was refused
         return _collect(outs, status, n)
 
     def measure_files_batch(self, ref_paths: list[str], deg_paths: list[str], num_threads: int = 0):
@@ -550,3 +582,29 @@ class Server:
         st = ServeStats()
         _check(lib.visqol_b200_server_stats(self._handle, ctypes.byref(st), int(bool(reset))))
         return {name: getattr(st, name) for name, _ in ServeStats._fields_}
+
+
+class Prepared:
+    """Owns a ``visqol_b200_prepared`` (see Context.prepare)."""
+
+    def __init__(self, ctx: Context, refs, sample_rate: int, device_inputs: bool, ref_lens):
+        n = len(refs)
+        if device_inputs:
+            rp = (c_void_p * n)(*refs)
+            rl = (c_size_t * n)(*ref_lens)
+        else:
+            refs = [np.ascontiguousarray(r, dtype=np.float64) for r in refs]
+            rp = (c_void_p * n)(*[r.ctypes.data for r in refs])
+            rl = (c_size_t * n)(*[r.size for r in refs])
+        handle = c_void_p()
+        _check(lib.visqol_b200_prepare(ctx._handle, n, rp, rl, sample_rate, DEVICE_INPUTS if device_inputs else 0,
+                                       ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            lib.visqol_b200_prepared_free(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()

@@ -75,6 +75,29 @@ int visqol_b200_measure_batch(visqol_ctx *ctx, size_t n,
 void visqol_b200_trace_free(visqol_b200_trace *trace);
 int visqol_b200_last_timing(visqol_ctx *ctx, visqol_b200_timing *out);
 
+/* ---- prepared references ---------------------------------------------------
+ * The reference-side work (samples, envelope statistics and spectrogram on
+ * the device; patch indices, VAD in speech mode) done once for references
+ * that are scored against many degraded signals (the reference's
+ * backend.Engine.prepare / measurePrepared, src/backend.zig:84-97,
+ * src/visqol.zig:194-244). Prepared with one context; usable by any context
+ * of the same device, mode and precision. Results equal those of
+ * visqol_measure_batch on the same pairs. */
+typedef struct visqol_b200_prepared visqol_b200_prepared;
+
+/* flags: VISQOL_B200_DEVICE_INPUTS (refs are device pointers). A reference
+ * that cannot be scored (too short, no patches) makes every pair scored
+ * against it fail with its code. */
+int visqol_b200_prepare(visqol_ctx *ctx, size_t n, const double *const *refs, const size_t *ref_lens,
+                        uint32_t sample_rate, uint32_t flags, visqol_b200_prepared **out);
+/* degs[i] against prepared reference ref_index[i] (ref_index NULL: i), as
+ * visqol_measure_batch: out[i] NULL and status[i] set on failure, the first
+ * error returned. flags: VISQOL_B200_DEVICE_INPUTS (degs on the device). */
+int visqol_b200_measure_prepared(visqol_ctx *ctx, const visqol_b200_prepared *prepared, size_t n,
+                                 const size_t *ref_index, const double *const *degs, const size_t *deg_lens,
+                                 uint32_t flags, visqol_result **out, int32_t *status);
+void visqol_b200_prepared_free(visqol_b200_prepared *prepared);
+
 /* ---- request server: continuous batching on one GPU ---------------------
  * No counterpart in the reference (its batch call is synchronous). Requests
  * are submitted one at a time from any thread and complete asynchronously.
