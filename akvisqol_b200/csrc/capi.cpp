@@ -12,6 +12,7 @@
 #include <exception>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -257,7 +258,7 @@ int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *
 void vqb::set_last_error(const std::string &message) { set_error(message); }
 
 int vqb::engine_options(const visqol_options &o, Options *opt, std::shared_ptr<const host::Svr> *svr,
-                        std::string *message) {
+                        std::shared_ptr<const host::LatticeMapper> *lattice, std::string *message) {
     // EXACT (and AUTO, which resolves to exact on a device with native f64)
     // reproduce the CPU path; FAST runs the gammatone's later stages in f32;
     // BALANCED keeps f64 throughout but with FMA and reassociated sums.
@@ -269,10 +270,12 @@ int vqb::engine_options(const visqol_options &o, Options *opt, std::shared_ptr<c
     opt->unscaled_speech = o.use_unscaled_speech_mos_mapping != 0;
     opt->disable_global_alignment = o.disable_global_alignment != 0;
     opt->disable_realignment = o.disable_realignment != 0;
+    (void)message;
     if (opt->speech && o.use_lattice_model) {
-        *message = "UnsupportedOp: the TF-Lattice speech mapper is not in this build; "
-                   "set use_lattice_model = 0 for the exponential mapping";
-        return VISQOL_E_MODEL;
+        // model_path names the lattice model in speech mode (reference src/capi.zig:189-203)
+        const std::string bytes =
+            (o.model_path && o.model_path[0]) ? host::read_file(o.model_path) : host::default_lattice_bytes();
+        *lattice = std::make_shared<host::LatticeMapper>(bytes, 21);
     }
     if (!opt->speech) {
         const std::string text =
@@ -343,11 +346,13 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
     auto c = std::make_unique<visqol_ctx>();
     try {
         std::string msg;
-        if (int rc = vqb::engine_options(o, &c->opt, &c->svr, &msg)) return fail(rc, msg);
+        std::shared_ptr<const vqb::host::LatticeMapper> lattice;
+        if (int rc = vqb::engine_options(o, &c->opt, &c->svr, &lattice, &msg)) return fail(rc, msg);
         int dev = 0;
         if (int rc = vqb::context_device(&dev, &msg)) return fail(rc, msg);
         const int lanes = vqb::env_lanes(2);
-        for (int l = 0; l < lanes; ++l) c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr));
+        for (int l = 0; l < lanes; ++l)
+            c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr, lattice));
     } catch (const Error &e) {
         return fail(e.code, e.what());
     } catch (const std::bad_alloc &) {
@@ -531,6 +536,32 @@ int visqol_b200_measure_prepared(visqol_ctx *c, const visqol_b200_prepared *p, s
     }
     return run_batch(c, n, rp.data(), rl.data(), degs, deg_lens, p->sample_rate,
                      (flags & VISQOL_B200_DEVICE_INPUTS) != 0, out, status, nullptr, prep.data());
+}
+
+int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double *fvnsim, const double *fvnsim10,
+                                const double *fstdnsim, const double *fvdegenergy, double *mos) {
+    if (!fvnsim || !fvnsim10 || !fstdnsim || !fvdegenergy || !mos || nb == 0)
+        return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    try {
+        static std::mutex mu;
+        static std::map<std::pair<std::string, size_t>, std::shared_ptr<const vqb::host::LatticeMapper>> cache;
+        const std::string path = model_path ? model_path : "";
+        std::shared_ptr<const vqb::host::LatticeMapper> m;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto &slot = cache[{path, nb}];
+            if (!slot)
+                slot = std::make_shared<vqb::host::LatticeMapper>(
+                    path.empty() ? vqb::host::default_lattice_bytes() : vqb::host::read_file(path), nb);
+            m = slot;
+        }
+        *mos = m->predict(fvnsim, fvnsim10, fstdnsim, fvdegenergy);
+        return VISQOL_OK;
+    } catch (const Error &e) {
+        return fail(e.code, e.what());
+    } catch (const std::exception &e) {
+        return fail(VISQOL_E_INTERNAL, e.what());
+    }
 }
 
 void visqol_b200_trace_free(visqol_b200_trace *t) {

@@ -15,8 +15,10 @@ visqol_result *box_result(host::Scores &&s);
 
 // Checks visqol_options and turns them into engine options and the SVR
 // model (audio mode); returns VISQOL_OK or an error code with *message.
+// In speech mode with use_lattice_model, *lattice gets the TF-Lattice
+// mapper (model_path's .tflite file, or the bundled model).
 int engine_options(const visqol_options &o, Options *opt, std::shared_ptr<const host::Svr> *svr,
-                   std::string *message);
+                   std::shared_ptr<const host::LatticeMapper> *lattice, std::string *message);
 
 // The device of new contexts and servers (VISQOL_CUDA_DEVICE, default 0),
 // or an error code with *message.

@@ -19,6 +19,8 @@
 //
 // Signals and intermediate spectrograms stay in HBM; only lags, energies,
 // matches and statistics cross to the host.
+#include <thread>
+
 #include "engine.h"
 
 #include <algorithm>
@@ -105,8 +107,9 @@ void *PinnedArena::alloc(size_t bytes) {
 // ---------------------------------------------------------------------------
 // Engine
 // ---------------------------------------------------------------------------
-Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr)
-    : device_(device), opt_(opt), svr_(std::move(svr)) {
+Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr,
+               std::shared_ptr<const host::LatticeMapper> lattice)
+    : device_(device), opt_(opt), svr_(std::move(svr)), lattice_(std::move(lattice)) {
     nb_ = opt.speech ? 21 : 32;
     patch_ = opt.speech ? 20 : 30;
     max_freq_ = opt.speech ? 8000.0 : -1.0;
@@ -967,23 +970,39 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         timing_.gammatone_kernel_ms += elapsed(gt_events_[2 * g], gt_events_[2 * g + 1]);
     timing_.kernel_launches = launch_counter() - launches0;
 
-    for (size_t i = 0; i < n; ++i) {
+    auto finish = [&](size_t i) {
         PairState &s = ps[i];
         PairOutcome &o = out[i];
         if (!s.live) {
             o.code = s.code;
             o.message = s.msg;
-            continue;
+            return;
         }
         try {
             s.trace.n_rms_window = W;
             o.scores = host::build_scores(std::move(s.matches), NB, fd, svr_.get(), opt_.speech, opt_.unscaled_speech,
-                                          rc.fb.cf, s.al.lag_seconds);
+                                          rc.fb.cf, s.al.lag_seconds, lattice_.get());
             o.trace = std::move(s.trace);
         } catch (const Error &e) {
             o.code = e.code;
             o.message = e.what();
+        } catch (const std::exception &e) {
+            o.code = kInternal;
+            o.message = e.what();
         }
+    };
+    // The lattice mapping runs a few milliseconds of host interpreter per
+    // pair: spread it over host threads (results are per pair).
+    const size_t workers = lattice_ ? std::min<size_t>(n, std::max(1u, std::thread::hardware_concurrency() / 2)) : 1;
+    if (workers > 1) {
+        std::vector<std::thread> pool;
+        for (size_t w = 0; w < workers; ++w)
+            pool.emplace_back([&, w] {
+                for (size_t i = w; i < n; i += workers) finish(i);
+            });
+        for (auto &t : pool) t.join();
+    } else {
+        for (size_t i = 0; i < n; ++i) finish(i);
     }
     timing_.total_ms = elapsed(events_[0], events_[7]);
     timing_.lag_ms = elapsed(events_[0], events_[1]);

@@ -110,7 +110,8 @@ struct PreparedRef {
 
 class Engine {
 public:
-    Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr);
+    Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> svr,
+           std::shared_ptr<const host::LatticeMapper> lattice = nullptr);
     ~Engine();
     Engine(const Engine &) = delete;
     Engine &operator=(const Engine &) = delete;
@@ -177,6 +178,7 @@ private:
     int device_;
     Options opt_;
     std::shared_ptr<const host::Svr> svr_;
+    std::shared_ptr<const host::LatticeMapper> lattice_;
     size_t nb_, patch_;
     double max_freq_;
     cudaStream_t stream_ = nullptr;

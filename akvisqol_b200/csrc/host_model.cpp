@@ -467,7 +467,8 @@ const std::string &default_svr_text() {
 }
 
 Scores build_scores(std::vector<Match> matches, size_t nb, double frame_duration, const Svr *svr, bool speech,
-                    bool unscaled_speech, const std::vector<double> &cf, double lag_s) {
+                    bool unscaled_speech, const std::vector<double> &cf, double lag_s,
+                    const LatticeMapper *lattice) {
     Scores s;
     const size_t n = matches.size();
     const double nf = (double)n;
@@ -517,6 +518,9 @@ Scores build_scores(std::vector<Match> matches, size_t nb, double frame_duration
     double mos;
     if (!speech) {
         mos = std::min(std::max(svr->predict(s.fvnsim.data()), 1.0), 5.0);
+    } else if (lattice) {
+        // widened without clamping, as the reference (src/lattice.zig:4-6)
+        mos = lattice->predict(s.fvnsim.data(), s.fvnsim10.data(), s.fstdnsim.data(), s.fvdegenergy.data());
     } else {
         // Exponential fit over mean NSIM (reference src/visqol.zig:85-96).
         double acc = 0.0;

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <stdexcept>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -131,8 +132,25 @@ struct Scores {
 
 // buildResult (reference src/visqol.zig:595-709) with QualityMapper.predict
 // (src/visqol.zig:81-98): SVR in audio mode, the exponential fit in speech.
+// Speech-mode TF-Lattice mapping (reference src/lattice.zig:14-71). The
+// model bytes are parsed once; predict is const and thread-safe.
+class LatticeMapper {
+public:
+    LatticeMapper(const std::string &model_bytes, size_t nb);
+    ~LatticeMapper();
+    double predict(const double *fvnsim, const double *fvnsim10, const double *fstdnsim,
+                   const double *fvdegenergy) const;
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+const std::string &default_lattice_bytes();
+
+// lattice: the speech-mode mapping when set (else the exponential fit).
 Scores build_scores(std::vector<Match> matches, size_t nb, double frame_duration, const Svr *svr, bool speech,
-                    bool unscaled_speech, const std::vector<double> &cf, double lag_s);
+                    bool unscaled_speech, const std::vector<double> &cf, double lag_s,
+                    const LatticeMapper *lattice = nullptr);
 
 // decodeWavAsMono (reference src/audio.zig:48-129).
 std::vector<double> decode_wav(const std::string &bytes, uint32_t *sample_rate);

@@ -74,6 +74,7 @@ struct visqol_b200_server {
     int device = 0;
     vqb::Options opt[2];  // audio, speech
     std::shared_ptr<const vqb::host::Svr> svr;
+    std::shared_ptr<const vqb::host::LatticeMapper> lattice;  // speech requests, when enabled
     uint64_t budget = 0, lane_budget = 0;
     uint32_t max_batch = 64;
 
@@ -96,7 +97,8 @@ struct visqol_b200_server {
 
     vqb::Engine &engine(Lane &l, uint32_t mode) {
         auto &e = l.engine[mode];
-        if (!e) e = std::make_unique<vqb::Engine>(device, opt[mode], mode == 0 ? svr : nullptr);
+        if (!e) e = std::make_unique<vqb::Engine>(device, opt[mode], mode == 0 ? svr : nullptr,
+                                                  mode == 0 ? nullptr : lattice);
         return *e;
     }
 
@@ -222,9 +224,10 @@ int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serv
         visqol_options audio = o, speech = o;
         audio.mode = VISQOL_MODE_AUDIO;
         speech.mode = VISQOL_MODE_SPEECH;
-        if (int rc = vqb::engine_options(audio, &s->opt[0], &s->svr, &msg)) return fail(rc, msg);
+        std::shared_ptr<const vqb::host::LatticeMapper> no_lattice;
+        if (int rc = vqb::engine_options(audio, &s->opt[0], &s->svr, &no_lattice, &msg)) return fail(rc, msg);
         std::shared_ptr<const vqb::host::Svr> none;
-        if (int rc = vqb::engine_options(speech, &s->opt[1], &none, &msg)) return fail(rc, msg);
+        if (int rc = vqb::engine_options(speech, &s->opt[1], &none, &s->lattice, &msg)) return fail(rc, msg);
         if (int rc = vqb::context_device(&s->device, &msg)) return fail(rc, msg);
         VQB_CUDA(cudaSetDevice(s->device));
         size_t free_b = 0, total_b = 0;

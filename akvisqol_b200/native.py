@@ -150,6 +150,7 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_dp_static": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
         "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
         "visqol_b200_peak": (c_int, [c_int, D]),
+        "visqol_b200_lattice_predict": (c_int, [c_char_p, c_size_t, D, D, D, D, D]),
         "visqol_b200_prepare": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, c_uint32, c_uint32,
                                         POINTER(c_void_p)]),
         "visqol_b200_measure_prepared": (c_int, [c_void_p, c_void_p, c_size_t, SZ, POINTER(c_void_p), SZ, c_uint32,
@@ -188,6 +189,7 @@ EXPORTS = [
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
+    "visqol_b200_lattice_predict",
     "visqol_b200_prepare", "visqol_b200_measure_prepared", "visqol_b200_prepared_free",
     "visqol_b200_server_create", "visqol_b200_server_destroy", "visqol_b200_server_submit",
     "visqol_b200_server_next", "visqol_b200_server_stats",
@@ -608,3 +610,12 @@ class Prepared:
 
     def __del__(self):
         self.close()
+
+
+def lattice_predict(fvnsim, fvnsim10, fstdnsim, fvdegenergy, model_path: str | None = None) -> float:
+    """Speech-mode TF-Lattice MOS of one set of per-band features (host only)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fvnsim, fvnsim10, fstdnsim, fvdegenergy)]
+    mos = c_double()
+    _check(lib.visqol_b200_lattice_predict(os.fsencode(model_path) if model_path else None, arrs[0].size,
+                                           *[_ptr(a) for a in arrs], ctypes.byref(mos)))
+    return mos.value

@@ -129,8 +129,9 @@ typedef struct {
 } visqol_b200_serve_stats;
 
 /* Server for the options' precision, radius and flags; `mode` of opts is
- * ignored (each request names its own). Speech requests need
- * use_lattice_model = 0. */
+ * ignored (each request names its own). Speech requests are mapped with the
+ * TF-Lattice model when use_lattice_model is set, else the exponential fit;
+ * model_path applies to the lattice model when it is set, else to the SVR. */
 int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serve_config *cfg,
                               visqol_b200_server **out);
 /* Stops taking requests, finishes those admitted, frees everything (results
@@ -154,6 +155,13 @@ int visqol_b200_server_next(visqol_b200_server *s, int32_t timeout_ms, uint64_t 
 /* Counters and latency percentiles; reset != 0 clears the latency samples
  * and the batch counters after reading. */
 int visqol_b200_server_stats(visqol_b200_server *s, visqol_b200_serve_stats *out, int reset);
+
+/* The speech-mode TF-Lattice MOS mapping alone, on the host (reference
+ * src/lattice.zig:14-71): nb values per feature; model_path NULL or "" for
+ * the bundled model. No GPU needed. */
+int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double *fvnsim,
+                                const double *fvnsim10, const double *fstdnsim,
+                                const double *fvdegenergy, double *mos);
 
 /* Device name, SM count and compute capability of the context's GPU. */
 int visqol_b200_device_info(int device, char *name, size_t name_len,

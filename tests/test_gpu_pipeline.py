@@ -182,3 +182,22 @@ def test_timing_counters(native, audio_ctx):
     assert t["total_ms"] > 0 and t["gammatone_kernel_ms"] > 0
     assert t["gammatone_launches"] >= 1 and t["kernel_launches"] > 10
     assert t["gammatone_window"] == 3840
+
+
+@pytest.mark.parametrize("precision", ["exact", "fast"])
+def test_speech_lattice_mapping(native, oracle, precision):
+    """Speech mode with the TF-Lattice mapper (the C ABI's default): the
+    pipeline's features mapped by the numpy restatement of the lattice."""
+    from akvisqol_b200 import synth
+    from oracle.lattice import Lattice
+    pairs = synth.speech_batch(4, min_s=2.0, max_s=5.0)
+    ctx = native.Context(mode=native.MODE_SPEECH, use_lattice_model=True, precision=precision)
+    got = run(ctx, pairs, 16000)
+    lat = Lattice()
+    for (code, res, _), (ref, deg) in zip(got, pairs):
+        assert code == 0
+        want, _ = oracle.measure(ref, deg, 16000, oracle.options(mode=1))
+        mos = lat.predict(want["fvnsim"], want["fvnsim10"], want["fstdnsim"], want["fvdegenergy"])
+        if want["vnsim"] < 0.15:
+            mos = 1.0
+        assert abs(res["moslqo"] - mos) <= (2e-6 if precision == "exact" else 1e-4), (res["moslqo"], mos)

@@ -20,11 +20,14 @@ SHIM = ROOT / "tests" / "native" / "build" / "libhost_shim.so"
 @pytest.fixture(scope="module")
 def hs():
     SHIM.parent.mkdir(parents=True, exist_ok=True)
-    srcs = [SHIM_SRC, ROOT / "akvisqol_b200" / "csrc" / "host_model.cpp"]
+    csrc = ROOT / "akvisqol_b200" / "csrc"
+    srcs = [SHIM_SRC, csrc / "host_model.cpp", csrc / "lattice.cpp", csrc / "tflite.cpp"]
     if not SHIM.is_file() or any(s.stat().st_mtime > SHIM.stat().st_mtime for s in srcs):
         model = ROOT / "akvisqol_b200" / "model" / "libsvm_nu_svr_model.txt"
-        subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
-                        "-I/usr/local/cuda/include", f"-DVQB_MODEL_PATH={model}", "-o", str(SHIM)]
+        lattice = next((ROOT / "akvisqol_b200" / "model").glob("lattice_*.tflite"))
+        subprocess.run(["g++", "-std=c++17", "-O2", "-march=x86-64-v3", "-fPIC", "-shared", "-ffp-contract=off",
+                        "-fno-fast-math", "-I/usr/local/cuda/include", f"-DVQB_MODEL_PATH={model}",
+                        f"-DVQB_LATTICE_PATH={lattice}", "-o", str(SHIM)]
                        + [str(s) for s in srcs], check=True)
     lib = ctypes.CDLL(str(SHIM))
     D, I64, SZ = POINTER(c_double), POINTER(c_int64), POINTER(c_size_t)
