@@ -224,6 +224,8 @@ int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serv
         visqol_options audio = o, speech = o;
         audio.mode = VISQOL_MODE_AUDIO;
         speech.mode = VISQOL_MODE_SPEECH;
+        // one model_path: the lattice model's when speech uses the lattice, else the SVR's
+        if (o.use_lattice_model) audio.model_path = nullptr;
         std::shared_ptr<const vqb::host::LatticeMapper> no_lattice;
         if (int rc = vqb::engine_options(audio, &s->opt[0], &s->svr, &no_lattice, &msg)) return fail(rc, msg);
         std::shared_ptr<const vqb::host::Svr> none;
