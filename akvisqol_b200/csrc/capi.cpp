@@ -564,6 +564,21 @@ int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double 
     }
 }
 
+int visqol_b200_autotune_choices(int32_t *rows, size_t max_rows, size_t *n_rows) {
+    if (!n_rows) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL argument");
+    const auto all = vqb::autotune_choices();
+    *n_rows = all.size();
+    for (size_t i = 0; i < all.size() && i < max_rows && rows; ++i) {
+        int32_t *r = rows + 5 * i;
+        r[0] = std::get<0>(all[i]);
+        r[1] = std::get<1>(all[i]);
+        r[2] = std::get<2>(all[i]);
+        r[3] = std::get<3>(all[i]);
+        r[4] = std::get<4>(all[i]);
+    }
+    return VISQOL_OK;
+}
+
 void visqol_b200_trace_free(visqol_b200_trace *t) {
     if (!t) return;
     delete reinterpret_cast<TraceBox *>(t);

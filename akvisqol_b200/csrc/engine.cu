@@ -20,6 +20,11 @@
 // Signals and intermediate spectrograms stay in HBM; only lags, energies,
 // matches and statistics cross to the host.
 #include <thread>
+#include <cstdlib>
+#include <map>
+#include <tuple>
+#include <mutex>
+#include <functional>
 
 #include "engine.h"
 
@@ -300,33 +305,116 @@ uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const Rat
     const int nbi = (int)nb_;
     const int W = (int)rc.geo.window, H = (int)rc.geo.hop;
     SpecJob *d_jobs = upload(jobs);
-    const int F = opt_.form == kFormF32 ? gammatone_fast_frames_per_cta() : gammatone_frames_per_cta(nbi);
-    const size_t tsz = gammatone_tile_size();
-    std::vector<char> tiles;
-    int ntiles = 0;
     uint64_t rms = 0;
-    for (size_t j = 0; j < jobs.size(); ++j) {
-        rms += (uint64_t)jobs[j].nf * nb_;
-        for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
-            tiles.resize(tiles.size() + tsz);
-            fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+    for (const SpecJob &j : jobs) rms += (uint64_t)j.nf * nb_;
+    // Tiles of F frames (the FP32 kernel's shape is fixed), uploaded on the
+    // main stream; a side stream waits for them.
+    auto tiles_of = [&](int F, int *ntiles) {
+        const size_t tsz = gammatone_tile_size();
+        std::vector<char> tiles;
+        *ntiles = 0;
+        for (size_t j = 0; j < jobs.size(); ++j)
+            for (int64_t f = 0; f < jobs[j].nf; f += F, ++*ntiles) {
+                tiles.resize(tiles.size() + tsz);
+                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+            }
+        void *d = upload_bytes(tiles.data(), tiles.size());
+        if (st != stream_) {
+            record(ev_inputs_);
+            VQB_CUDA(cudaStreamWaitEvent(st, ev_inputs_, 0));
         }
-    }
-    void *d_tiles = upload_bytes(tiles.data(), tiles.size());
-    if (st != stream_) {
-        // job tables were copied on the main stream
-        record(ev_inputs_);
-        VQB_CUDA(cudaStreamWaitEvent(st, ev_inputs_, 0));
-    }
-    if (begin) VQB_CUDA(cudaEventRecord(begin, st));
-    if (opt_.form == kFormF32)
+        return d;
+    };
+    auto launch_frames = [&](int F) {
+        int ntiles = 0;
+        const void *d_tiles = tiles_of(F, &ntiles);
+        if (opt_.form == kFormF64)
+            launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, F, st);
+        else
+            launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, W, H, F, st);
+    };
+    if (opt_.form == kFormF32) {
+        int ntiles = 0;
+        const void *d_tiles = tiles_of(gammatone_fast_frames_per_cta(), &ntiles);
+        if (begin) VQB_CUDA(cudaEventRecord(begin, st));
         launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
-    else if (opt_.form == kFormF64)
-        launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
-    else
-        launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, W, H, st);
+    } else {
+        const int F = tuned(kTuneGammatone, opt_.form, nbi, gammatone_frames_candidates(nbi), launch_frames, st);
+        int ntiles = 0;
+        const void *d_tiles = tiles_of(F, &ntiles);
+        if (begin) VQB_CUDA(cudaEventRecord(begin, st));
+        if (opt_.form == kFormF64)
+            launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, F, st);
+        else
+            launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, W, H, F, st);
+    }
     if (end) VQB_CUDA(cudaEventRecord(end, st));
     return rms;
+}
+
+namespace {
+
+// Launch shapes chosen by measurement, per (device, kernel, variant): shared
+// by every engine of the process. VISQOL_AUTOTUNE=0 keeps the defaults.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune;
+
+bool autotune_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("VISQOL_AUTOTUNE");
+        return !e || std::atoi(e) != 0;
+    }();
+    return on;
+}
+
+}  // namespace
+
+int Engine::tuned(int kernel, int a, int b, const std::vector<int> &candidates,
+                  const std::function<void(int)> &launch, cudaStream_t st) {
+    if (!autotune_enabled() || candidates.size() < 2) return candidates.at(0);
+    const auto key = std::make_tuple(device_, kernel, a, b);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) return it->second;
+    }
+    // The candidates run on this batch's real jobs (the kernels write the
+    // same values whatever their shape), one warm-up each, then three timed
+    // rounds in turn so that other work on the GPU touches them alike; each
+    // keeps its fastest run. A candidate replaces the default only when it is
+    // at least 3% faster.
+    cudaEvent_t e0, e1;
+    VQB_CUDA(cudaEventCreate(&e0));
+    VQB_CUDA(cudaEventCreate(&e1));
+    std::vector<float> best_ms(candidates.size(), 0.0f);
+    for (int c : candidates) launch(c);
+    for (int round = 0; round < 3; ++round)
+        for (size_t i = 0; i < candidates.size(); ++i) {
+            VQB_CUDA(cudaEventRecord(e0, st));
+            launch(candidates[i]);
+            VQB_CUDA(cudaEventRecord(e1, st));
+            VQB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            VQB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (round == 0 || ms < best_ms[i]) best_ms[i] = ms;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int best = candidates[0];
+    float best_t = best_ms[0] * 0.97f;
+    for (size_t i = 1; i < candidates.size(); ++i)
+        if (best_ms[i] < best_t) best = candidates[i], best_t = best_ms[i];
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    return g_tune.emplace(key, best).first->second;
+}
+
+std::vector<std::tuple<int, int, int, int, int>> autotune_choices() {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    std::vector<std::tuple<int, int, int, int, int>> out;
+    for (const auto &kv : g_tune)
+        out.emplace_back(std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first),
+                         kv.second);
+    return out;
 }
 
 PreparedRef::~PreparedRef() {
@@ -463,7 +551,7 @@ void Engine::spectrogram(const host::Filterbank &fb, const double *d_hann, size_
         fill_gammatone_tile(tiles.data() + tiles.size() - tsz, 0, (int)f);
     }
     void *d_tiles = upload_bytes(tiles.data(), tiles.size());
-    launch_gammatone(d_job, d_tiles, ntiles, d_coeffs, nbi, d_hann, (int)window, (int)hop, stream_);
+    launch_gammatone(d_job, d_tiles, ntiles, d_coeffs, nbi, d_hann, (int)window, (int)hop, F, stream_);
     sync();
 }
 
@@ -664,11 +752,10 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     std::vector<PrepJob> prep_jobs;
     std::vector<PlaneJob> plane_jobs;
     std::vector<RefTermsJob> term_jobs;
-    std::vector<TableTask> tasks;
+    std::vector<TableTask> table_rows;  // one per patch: offsets [off0, hi]
     std::vector<DpJob> dp_jobs;
     std::vector<StatsJob> stat_jobs;
     int max_width = 0;
-    const int per_cta = table_offsets_per_cta();
     for (size_t i = 0; i < n; ++i) {
         PairState &s = ps[i];
         if (!s.live) continue;
@@ -746,9 +833,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         for (size_t p = 0; p < np; ++p) {
             double *terms = s.terms + p * 4 * NB * P;
             term_jobs.push_back(RefTermsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], terms});
-            for (int64_t off0 = s.search.lo[p]; off0 <= s.search.hi[p]; off0 += per_cta)
-                tasks.push_back(TableTask{terms, s.pad, s.mu, s.dms, s.sds, (int32_t)s.width, (int32_t)off0,
-                                          (int32_t)s.search.hi[p], s.sims + p * s.nf_deg});
+            table_rows.push_back(TableTask{terms, s.pad, s.mu, s.dms, s.sds, (int32_t)s.width,
+                                           (int32_t)s.search.lo[p], (int32_t)s.search.hi[p], s.sims + p * s.nf_deg});
             s.trace.n_cells += (uint64_t)(s.search.hi[p] - s.search.lo[p] + 1) * NB * P;
             double *ms = s.mstats + p * (3 * NB + 1);
             stat_jobs.push_back(StatsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], s.deg_prep,
@@ -769,7 +855,21 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     record(events_[4]);
     if (!plane_jobs.empty()) launch_plane(upload(plane_jobs), (int)plane_jobs.size(), nbi, max_width, stream_);
     if (!term_jobs.empty()) launch_ref_terms(upload(term_jobs), (int)term_jobs.size(), nbi, (int)P, stream_);
-    if (!tasks.empty()) launch_table(upload(tasks), (int)tasks.size(), nbi, (int)P, opt_.form != kFormExact, stream_);
+    if (!table_rows.empty()) {
+        const bool fast_cells = opt_.form != kFormExact;
+        auto launch_width = [&](int w) {
+            std::vector<TableTask> tasks;
+            for (const TableTask &row : table_rows)
+                for (int64_t off0 = row.off0; off0 <= row.hi; off0 += w) {
+                    TableTask t = row;
+                    t.off0 = (int32_t)off0;
+                    tasks.push_back(t);
+                }
+            launch_table(upload(tasks), (int)tasks.size(), nbi, (int)P, fast_cells, w, stream_);
+        };
+        const int w = tuned(kTuneTable, fast_cells ? 1 : 0, nbi, table_width_candidates(), launch_width, stream_);
+        launch_width(w);
+    }
     if (!dp_jobs.empty()) launch_dp(upload(dp_jobs), (int)dp_jobs.size(), stream_);
     if (!stat_jobs.empty()) launch_stats(upload(stat_jobs), (int)stat_jobs.size(), nbi, stream_);
     std::vector<int64_t *> h_offs(n, nullptr);

@@ -3,6 +3,8 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
+#include <tuple>
 #include <map>
 #include <memory>
 #include <string>
@@ -158,6 +160,12 @@ private:
     };
     // Envelope statistics of sum jobs: serial (exact) or tree (fast).
     void launch_sums(const std::vector<SumJob> &sums);
+    // The launch shape for a kernel class among candidates: measured on the
+    // caller's jobs at first use per device (launch(c) launches them with
+    // shape c on st), then reused; candidates[0] when autotuning is off.
+    enum TuneKernel { kTuneGammatone = 0, kTuneTable = 1 };
+    int tuned(int kernel, int a, int b, const std::vector<int> &candidates, const std::function<void(int)> &launch,
+              cudaStream_t st);
     // Gammatone spectrograms of the jobs in this engine's form on stream st;
     // returns the RMS count.
     uint64_t launch_spectrograms(const std::vector<SpecJob> &jobs, const RateCache &rc, cudaStream_t st,
@@ -192,6 +200,10 @@ private:
     cudaEvent_t gt_events_[6] = {};  // begin/end of up to three gammatone launches
     Timing timing_;
 };
+
+// The autotuner's choices so far: (device, kernel, variant a, variant b,
+// chosen shape).
+std::vector<std::tuple<int, int, int, int, int>> autotune_choices();
 
 // CUDA call check: throws Error(kBackend) with the call and message.
 void cuda_check(cudaError_t e, const char *what);

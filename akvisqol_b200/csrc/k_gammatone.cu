@@ -72,13 +72,21 @@ __global__ void __launch_bounds__(256) copy_frames_kernel(const CopyJob *__restr
 }  // namespace
 
 int gammatone_frames_per_cta(int nb) { return 256 / nb; }
+
+std::vector<int> gammatone_frames_candidates(int nb) {
+    const int f = 256 / nb;
+    std::vector<int> c{f};
+    if (f / 2 >= 1) c.push_back(f / 2);
+    if (f / 4 >= 1) c.push_back(f / 4);
+    return c;
+}
 size_t gammatone_tile_size() { return sizeof(Tile); }
 void fill_gammatone_tile(void *dst, int job, int frame0) { *static_cast<Tile *>(dst) = Tile{job, frame0}; }
 
 void launch_gammatone(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const BandCoeffs *d_coeffs, int nb,
-                      const double *d_hann, int window, int hop, cudaStream_t s) {
+                      const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s) {
     if (ntiles <= 0) return;
-    const int threads = gammatone_frames_per_cta(nb) * nb;
+    const int threads = frames_per_cta * nb;
     gammatone_kernel<<<ntiles, threads, 0, s>>>(d_jobs, static_cast<const Tile *>(d_tiles), d_coeffs, nb, d_hann,
                                                window, hop);
     launch_counter() += 1;

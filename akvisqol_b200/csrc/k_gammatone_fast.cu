@@ -275,9 +275,9 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
 namespace vqb {
 
 void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                             int nb, const double *d_hann, int window, int hop, cudaStream_t s) {
+                             int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s) {
     if (ntiles <= 0) return;
-    const int threads = (256 / nb) * nb;
+    const int threads = frames_per_cta * nb;
     gammatone_f64fma_kernel<<<ntiles, threads, 0, s>>>(d_jobs, static_cast<const Tile *>(d_tiles), d_coeffs, nb,
                                                       d_hann, window, hop);
     launch_counter() += 1;

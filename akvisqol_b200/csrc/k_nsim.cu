@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) ref_terms_kernel(const RefTermsJob *__res
     }
 }
 
-constexpr int kTableThreads = 128;
+constexpr int kTableThreads = 128;  // default offsets per CTA
 
 // The fast forms' cell arithmetic: the 3x3 window as an FMA chain and the
 // cell's two quotients as one, (2 mr md + c1)(srd + c3) /
@@ -105,8 +105,8 @@ __device__ inline double taps(double a00, double a01, double a02, double a10, do
 }
 
 // One thread per (patch, offset); CTA = one patch x 128 offsets.
-template <bool kFast>
-__global__ void __launch_bounds__(kTableThreads) table_kernel(const TableTask *__restrict__ tasks, int nb, int P) {
+template <bool kFast, int kThreads>
+__global__ void __launch_bounds__(kThreads) table_kernel(const TableTask *__restrict__ tasks, int nb, int P) {
     extern __shared__ double sm[];
     const TableTask t = tasks[blockIdx.x];
     const int total = nb * P;
@@ -256,18 +256,33 @@ void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaS
 
 int table_offsets_per_cta() { return kTableThreads; }
 
+std::vector<int> table_width_candidates() { return {128, 64, 256}; }
+
 void nsim_init_attributes() {
-    cudaFuncSetAttribute(table_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(table_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_kernel<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, cudaStream_t s) {
+void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s) {
     if (ntasks <= 0) return;
     const size_t smem = (size_t)4 * nb * P * sizeof(double);
-    if (fast)
-        table_kernel<true><<<ntasks, kTableThreads, smem, s>>>(d_tasks, nb, P);
-    else
-        table_kernel<false><<<ntasks, kTableThreads, smem, s>>>(d_tasks, nb, P);
+#define VQB_TABLE(W)                                                             \
+    if (fast)                                                                    \
+        table_kernel<true, W><<<ntasks, W, smem, s>>>(d_tasks, nb, P);           \
+    else                                                                         \
+        table_kernel<false, W><<<ntasks, W, smem, s>>>(d_tasks, nb, P);
+    if (width == 64) {
+        VQB_TABLE(64)
+    } else if (width == 256) {
+        VQB_TABLE(256)
+    } else {
+        VQB_TABLE(128)
+    }
+#undef VQB_TABLE
     launch_counter() += 1;
 }
 

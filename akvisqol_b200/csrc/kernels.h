@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -114,10 +115,13 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
 
 // k_gammatone.cu
 int gammatone_frames_per_cta(int nb);
+// CTA shapes the autotuner may choose among for the exact and FP64 FMA
+// kernels (frames per CTA; the first is the default).
+std::vector<int> gammatone_frames_candidates(int nb);
 size_t gammatone_tile_size();
 void fill_gammatone_tile(void *dst, int job, int frame0);
 void launch_gammatone(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const BandCoeffs *d_coeffs, int nb,
-                      const double *d_hann, int window, int hop, cudaStream_t s);
+                      const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s);
 void launch_copy_frames(const CopyJob *d_jobs, int njobs, int nb, int max_cols, cudaStream_t s);
 
 // k_gammatone_fast.cu (tiles as fill_gammatone_tile writes them)
@@ -127,7 +131,7 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
                            int nb, const double *d_hann, int window, int hop, cudaStream_t s);
 // f64 FMA form: tiles of gammatone_frames_per_cta(nb) frames, as the exact kernel.
 void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                             int nb, const double *d_hann, int window, int hop, cudaStream_t s);
+                             int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s);
 
 // k_spec.cu
 void launch_prep(const PrepJob *d_jobs, int njobs, int nb, cudaStream_t s);
@@ -138,8 +142,11 @@ void nsim_init_attributes();
 void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cudaStream_t s);
 void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaStream_t s);
 int table_offsets_per_cta();
-// fast: the fast forms' cell arithmetic (FMA, one division per cell).
-void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, cudaStream_t s);
+// fast: the fast forms' cell arithmetic (FMA, one division per cell);
+// width: offsets per CTA, one of table_width_candidates() (the first is the
+// default); tasks must be built with the same width.
+std::vector<int> table_width_candidates();
+void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s);
 void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s);
 
 // k_dp.cu

@@ -177,7 +177,8 @@ int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref, const double *
         DBuf<vqb::TableTask> dtasks(tasks.data(), tasks.size());
         vqb::launch_plane(dpj.p, 1, (int)nb, (int)width, e.stream());
         vqb::launch_ref_terms(dtj.p, (int)tj.size(), (int)nb, (int)patch, e.stream());
-        vqb::launch_table(dtasks.p, (int)tasks.size(), (int)nb, (int)patch, false, e.stream());
+        vqb::launch_table(dtasks.p, (int)tasks.size(), (int)nb, (int)patch, false, vqb::table_offsets_per_cta(),
+                          e.stream());
         VQB_CUDA(cudaStreamSynchronize(e.stream()));
         sims.get(out, np * nf_deg);
     });

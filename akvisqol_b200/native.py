@@ -150,6 +150,7 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_dp_static": (c_int, [D, c_size_t, c_size_t, I64, I64, I64, U8, SZ]),
         "visqol_b200_patch_similarity": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D]),
         "visqol_b200_peak": (c_int, [c_int, D]),
+        "visqol_b200_autotune_choices": (c_int, [POINTER(c_int32), c_size_t, SZ]),
         "visqol_b200_lattice_predict": (c_int, [c_char_p, c_size_t, D, D, D, D, D]),
         "visqol_b200_prepare": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, c_uint32, c_uint32,
                                         POINTER(c_void_p)]),
@@ -189,7 +190,7 @@ EXPORTS = [
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
-    "visqol_b200_lattice_predict",
+    "visqol_b200_lattice_predict", "visqol_b200_autotune_choices",
     "visqol_b200_prepare", "visqol_b200_measure_prepared", "visqol_b200_prepared_free",
     "visqol_b200_server_create", "visqol_b200_server_destroy", "visqol_b200_server_submit",
     "visqol_b200_server_next", "visqol_b200_server_stats",
@@ -619,3 +620,14 @@ def lattice_predict(fvnsim, fvnsim10, fstdnsim, fvdegenergy, model_path: str | N
     _check(lib.visqol_b200_lattice_predict(os.fsencode(model_path) if model_path else None, arrs[0].size,
                                            *[_ptr(a) for a in arrs], ctypes.byref(mos)))
     return mos.value
+
+
+def autotune_choices() -> list[dict]:
+    """Launch shapes the autotuner chose in this process."""
+    n = c_size_t()
+    _check(lib.visqol_b200_autotune_choices(None, 0, ctypes.byref(n)))
+    rows = (c_int32 * (5 * max(1, n.value)))()
+    _check(lib.visqol_b200_autotune_choices(rows, n.value, ctypes.byref(n)))
+    names = {0: "gammatone_frames_per_cta", 1: "nsim_table_offsets_per_cta"}
+    return [{"device": rows[5 * i], "kernel": names.get(rows[5 * i + 1], str(rows[5 * i + 1])),
+             "variant": (rows[5 * i + 2], rows[5 * i + 3]), "choice": rows[5 * i + 4]} for i in range(n.value)]

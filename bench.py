@@ -492,6 +492,7 @@ def run_ours(args, rank, world, local):
         "forms": {f: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline": r["roofline"],
                       "failures": r["failures"]} for f, r in runs.items()},
         "prepared_references": prepared_line,
+        "autotune": native.autotune_choices(),
     }
     if args.config_pairs > 0 and rank == 0:
         line["uneven_batches"] = uneven_configs(native, torch, args.config_pairs, plain_value)

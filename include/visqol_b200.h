@@ -163,6 +163,14 @@ int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double 
                                 const double *fvnsim10, const double *fstdnsim,
                                 const double *fvdegenergy, double *mos);
 
+/* Launch shapes the autotuner has chosen in this process: *n_rows rows of
+ * {device, kernel (0 gammatone frames per CTA, 1 NSIM-table offsets per
+ * CTA), variant a (form / cell arithmetic), variant b (bands), choice},
+ * written to rows up to max_rows. Each kernel class is measured on its
+ * first batch per device (candidate shapes write identical results);
+ * VISQOL_AUTOTUNE=0 keeps the default shapes. */
+int visqol_b200_autotune_choices(int32_t *rows, size_t max_rows, size_t *n_rows);
+
 /* Device name, SM count and compute capability of the context's GPU. */
 int visqol_b200_device_info(int device, char *name, size_t name_len,
                             int *sm_count, int *cc_major, int *cc_minor);

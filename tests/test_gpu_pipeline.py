@@ -201,3 +201,16 @@ def test_speech_lattice_mapping(native, oracle, precision):
         if want["vnsim"] < 0.15:
             mos = 1.0
         assert abs(res["moslqo"] - mos) <= (2e-6 if precision == "exact" else 1e-4), (res["moslqo"], mos)
+
+
+def test_autotune_choices_are_candidates(native, audio_ctx):
+    from akvisqol_b200 import synth
+    ref, deg = synth.audio_pair(synth.SEED_BASE + 9, seconds=3.0)
+    run(audio_ctx, [(ref, deg)], 48000)
+    rows = native.autotune_choices()
+    assert rows, "no kernel was tuned"
+    for r in rows:
+        if r["kernel"] == "gammatone_frames_per_cta":
+            assert r["choice"] in (256 // r["variant"][1], 128 // r["variant"][1], 64 // r["variant"][1])
+        else:
+            assert r["choice"] in (64, 128, 256)
