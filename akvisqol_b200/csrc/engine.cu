@@ -339,7 +339,10 @@ uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const Rat
         if (begin) VQB_CUDA(cudaEventRecord(begin, st));
         launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
     } else {
-        const int F = tuned(kTuneGammatone, opt_.form, nbi, gammatone_frames_candidates(nbi), launch_frames, st);
+        const int F = tuned(kTuneGammatone, opt_.form, nbi,
+                            opt_.form == kFormF64 ? gammatone_f64fma_frames_candidates(nbi)
+                                                  : gammatone_frames_candidates(nbi),
+                            launch_frames, st);
         int ntiles = 0;
         const void *d_tiles = tiles_of(F, &ntiles);
         if (begin) VQB_CUDA(cudaEventRecord(begin, st));
@@ -822,7 +825,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         spec_jobs.push_back(SpecJob{VSig{s.deg_al, 0, s.al.len, s.al.len}, (int64_t)s.nf_deg, s.deg_raw});
         s.trace.n_rms += NB * (s.nf_ref + s.nf_deg);
         prep_jobs.push_back(PrepJob{s.ref_raw, s.deg_raw, s.ref_prep, s.deg_prep, (int32_t)s.nf_ref, (int32_t)s.nf_deg});
-        plane_jobs.push_back(PlaneJob{s.deg_prep, (int32_t)s.nf_deg, (int32_t)s.width, s.pad, s.mu, s.dms, s.sds});
+        plane_jobs.push_back(PlaneJob{s.deg_prep, (int32_t)s.nf_deg, (int32_t)s.width, s.pad, s.mu, s.dms, s.sds,
+                                      opt_.form != kFormExact ? 1 : 0});
         int64_t *d_lo = nullptr;
         {
             std::vector<int64_t> lohi(2 * np);
@@ -832,7 +836,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         }
         for (size_t p = 0; p < np; ++p) {
             double *terms = s.terms + p * 4 * NB * P;
-            term_jobs.push_back(RefTermsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], terms});
+            term_jobs.push_back(RefTermsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], terms,
+                                            opt_.form != kFormExact ? 1 : 0});
             table_rows.push_back(TableTask{terms, s.pad, s.mu, s.dms, s.sds, (int32_t)s.width,
                                            (int32_t)s.search.lo[p], (int32_t)s.search.hi[p], s.sims + p * s.nf_deg});
             s.trace.n_cells += (uint64_t)(s.search.hi[p] - s.search.lo[p] + 1) * NB * P;

@@ -37,9 +37,7 @@ __global__ void __launch_bounds__(256) gammatone_kernel(const SpecJob *__restric
     double sum_sq = 0;
     const int64_t k0 = f * hop;
     const VSig sig = job.sig;
-#pragma unroll 4
-    for (int i = 0; i < window; ++i) {
-        const double s = vsig_at(sig, k0 + i) * __ldg(hann + i);
+    auto step = [&](double s) {
         const double f1 = k.s1n0 * s + s1c0;
         s1c0 = k.s1n1 * s + s1c1 - k.d1 * f1;
         s1c1 = -(k.d2 * f1);
@@ -53,6 +51,24 @@ __global__ void __launch_bounds__(256) gammatone_kernel(const SpecJob *__restric
         s4c0 = k.s4n1 * f3 + s4c1 - k.d1 * f4;
         s4c1 = -(k.d2 * f4);
         sum_sq += f4 * f4;
+    };
+    if (nb == 32) {
+        // A warp is one frame's 32 bands: lane j forms windowed sample
+        // i0 + j once (coalesced loads, one multiply per 32 samples) and the
+        // warp reads it by shuffle, taking the product off the FP64 pipe.
+        const int lane = threadIdx.x & 31;
+        int i0 = 0;
+        for (; i0 + 32 <= window; i0 += 32) {
+            const double x = vsig_at(sig, k0 + i0 + lane) * __ldg(hann + i0 + lane);
+#pragma unroll 8
+            for (int j = 0; j < 32; ++j) step(__shfl_sync(0xffffffffu, x, j));
+        }
+        const int rest = window - i0;
+        const double x = lane < rest ? vsig_at(sig, k0 + i0 + lane) * __ldg(hann + i0 + lane) : 0.0;
+        for (int j = 0; j < rest; ++j) step(__shfl_sync(0xffffffffu, x, j));
+    } else {
+#pragma unroll 4
+        for (int i = 0; i < window; ++i) step(vsig_at(sig, k0 + i) * __ldg(hann + i));
     }
     const double inv_n = 1.0 / (double)window;
     job.out[(int64_t)band * job.nf + f] = sqrt(sum_sq * inv_n);

@@ -170,17 +170,13 @@ __global__ void __launch_bounds__(256) gammatone_fast_kernel(const SpecJob *__re
     if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post;
 }
 
-template <class Load>
-__device__ double cascade64(const Load &sample, int64_t k0, const FastBandCoeffs &kc, const double *__restrict__ hann,
-                            int window) {
-    const double b0 = kc.beta64[0], b1 = kc.beta64[1], b2 = kc.beta64[2], b3 = kc.beta64[3];
-    const double nd1 = -kc.d1, nd2 = -kc.d2;
+// Two frames per thread (the second hop samples later): two independent
+// recurrences give each warp twice the FP64 work between dependent steps.
+struct Cascade64 {
     double xp = 0.0, y1a = 0.0, y2a = 0.0, y1b = 0.0, y2b = 0.0, y1c = 0.0, y2c = 0.0, y1d = 0.0, y2d = 0.0;
     double acc = 0.0;
-#pragma unroll 4
-    for (int i = 0; i < window; ++i) {
-        const double x = sample(k0 + i) * __ldg(hann + i);
-        // stage k input v, previous input vp = stage k-1's previous output
+    __device__ inline void step(double x, double b0, double b1, double b2, double b3, double nd1, double nd2) {
+        // stage k input v, previous input = stage k-1's previous output
         const double ya = __fma_rn(nd1, y1a, __fma_rn(nd2, y2a, __fma_rn(b0, xp, x)));
         const double yb = __fma_rn(nd1, y1b, __fma_rn(nd2, y2b, __fma_rn(b1, y1a, ya)));
         const double yc = __fma_rn(nd1, y1c, __fma_rn(nd2, y2c, __fma_rn(b2, y1b, yb)));
@@ -196,33 +192,78 @@ __device__ double cascade64(const Load &sample, int64_t k0, const FastBandCoeffs
         y1d = yd;
         acc = __fma_rn(yd, yd, acc);
     }
-    return acc;
+};
+
+template <class Load>
+__device__ void cascade64x2(const Load &sample, int64_t ka, int64_t kb, const FastBandCoeffs &kc,
+                            const double *__restrict__ hann, int window, bool warp_frame, double &acc_a,
+                            double &acc_b) {
+    const double b0 = kc.beta64[0], b1 = kc.beta64[1], b2 = kc.beta64[2], b3 = kc.beta64[3];
+    const double nd1 = -kc.d1, nd2 = -kc.d2;
+    Cascade64 A, B;
+    if (warp_frame) {
+        // a warp holds two frames' 32 bands: lane j forms windowed samples
+        // i0 + j of both frames, shuffled to the warp
+        const int lane = threadIdx.x & 31;
+        int i0 = 0;
+        for (; i0 + 32 <= window; i0 += 32) {
+            const double h = __ldg(hann + i0 + lane);
+            const double xa = sample(ka + i0 + lane) * h, xb = sample(kb + i0 + lane) * h;
+#pragma unroll 8
+            for (int j = 0; j < 32; ++j) {
+                A.step(__shfl_sync(0xffffffffu, xa, j), b0, b1, b2, b3, nd1, nd2);
+                B.step(__shfl_sync(0xffffffffu, xb, j), b0, b1, b2, b3, nd1, nd2);
+            }
+        }
+        const int rest = window - i0;
+        const double h = lane < rest ? __ldg(hann + i0 + lane) : 0.0;
+        const double xa = lane < rest ? sample(ka + i0 + lane) * h : 0.0;
+        const double xb = lane < rest ? sample(kb + i0 + lane) * h : 0.0;
+        for (int j = 0; j < rest; ++j) {
+            A.step(__shfl_sync(0xffffffffu, xa, j), b0, b1, b2, b3, nd1, nd2);
+            B.step(__shfl_sync(0xffffffffu, xb, j), b0, b1, b2, b3, nd1, nd2);
+        }
+    } else {
+#pragma unroll 2
+        for (int i = 0; i < window; ++i) {
+            const double h = __ldg(hann + i);
+            A.step(sample(ka + i) * h, b0, b1, b2, b3, nd1, nd2);
+            B.step(sample(kb + i) * h, b0, b1, b2, b3, nd1, nd2);
+        }
+    }
+    acc_a = A.acc;
+    acc_b = B.acc;
 }
 
-__global__ void __launch_bounds__(256) gammatone_f64fma_kernel(const SpecJob *__restrict__ jobs,
+// CTA: F frames x nb bands, two frames per thread (threads = F/2 x nb).
+// Thread t: band t % nb, frames frame0 + 2 (t / nb) and the next.
+__global__ void __launch_bounds__(256, 2) gammatone_f64fma_kernel(const SpecJob *__restrict__ jobs,
                                                                const Tile *__restrict__ tiles,
                                                                const FastBandCoeffs *__restrict__ coeffs, int nb,
                                                                const double *__restrict__ hann, int window, int hop) {
     const Tile tile = tiles[blockIdx.x];
-    const int frames_per_cta = blockDim.x / nb;
-    const int fl = threadIdx.x / nb;
-    const int band = threadIdx.x - fl * nb;
-    if (fl >= frames_per_cta) return;
+    const int pair = threadIdx.x / nb;
+    const int band = threadIdx.x - pair * nb;
     const SpecJob job = jobs[tile.job];
-    const int64_t f = (int64_t)tile.frame0 + fl;
+    const int64_t f = (int64_t)tile.frame0 + 2 * pair;
     if (f >= job.nf) return;
     const FastBandCoeffs &kc = coeffs[band];
-    const int64_t k0 = f * hop;
+    const int64_t ka = f * hop, kb = ka + hop;
     const VSig sig = job.sig;
-    double acc;
-    if (window_inside(sig, k0, window))
-        acc = cascade64(Direct{sig.base - sig.head}, k0, kc, hann, window);
+    double acc_a, acc_b;
+    // With 32 bands a warp is one frame pair, and window_inside (over both
+    // frames) is the same for all its lanes, so the shuffles see the whole
+    // warp.
+    const bool warp_frame = nb == 32;
+    if (window_inside(sig, ka, hop + window))
+        cascade64x2(Direct{sig.base - sig.head}, ka, kb, kc, hann, window, warp_frame, acc_a, acc_b);
     else
-        acc = cascade64(Checked{sig}, k0, kc, hann, window);
+        cascade64x2(Checked{sig}, ka, kb, kc, hann, window, warp_frame, acc_a, acc_b);
     const double inv_n = 1.0 / (double)window;
-    job.out[(int64_t)band * job.nf + f] = sqrt(acc * inv_n) * kc.post64;
+    double *out = job.out + (int64_t)band * job.nf;
+    out[f] = sqrt(acc_a * inv_n) * kc.post64;
+    if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * kc.post64;
 }
-
 
 }  // namespace
 
@@ -274,10 +315,15 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
 
 namespace vqb {
 
+std::vector<int> gammatone_f64fma_frames_candidates(int nb) {
+    const int f = 2 * (256 / nb);  // two frames per thread, 256 threads
+    return {f, f / 2, f / 4};
+}
+
 void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
                              int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s) {
     if (ntiles <= 0) return;
-    const int threads = frames_per_cta * nb;
+    const int threads = (frames_per_cta / 2) * nb;
     gammatone_f64fma_kernel<<<ntiles, threads, 0, s>>>(d_jobs, static_cast<const Tile *>(d_tiles), d_coeffs, nb,
                                                       d_hann, window, hop);
     launch_counter() += 1;

@@ -19,6 +19,11 @@ namespace vqb {
 
 namespace {
 
+// sign(v) sqrt(|v|): the fast forms store variances as signed roots, so a
+// cell's sqrt(srs * sds) becomes a product of two stored roots (and
+// srs * sds < 0 exactly when the roots' product is negative).
+__device__ inline double signed_root(double v) { return v < 0.0 ? -sqrt(-v) : sqrt(v); }
+
 // Degraded plane of one pair: the prepared spectrogram zero-padded to
 // `width` frames, its 3x3 mean, mean² and variance (reference
 // src/nsim.zig:236-263). out arrays are nb x width.
@@ -41,7 +46,7 @@ __global__ void __launch_bounds__(256) plane_kernel(const PlaneJob *__restrict__
         job.pad[e] = p11;
         job.mu[e] = mu;
         job.dms[e] = dms;
-        job.sds[e] = csq - dms;
+        job.sds[e] = job.roots ? signed_root(csq - dms) : csq - dms;
     }
 }
 
@@ -65,7 +70,7 @@ __global__ void __launch_bounds__(256) ref_terms_kernel(const RefTermsJob *__res
         job.out[e] = p11;
         job.out[total + e] = mu;
         job.out[2 * total + e] = rms;
-        job.out[3 * total + e] = csq - rms;
+        job.out[3 * total + e] = job.roots ? signed_root(csq - rms) : csq - rms;
     }
 }
 
@@ -88,12 +93,13 @@ __device__ inline double taps9_fma(double a00, double a01, double a02, double a1
     return __fma_rn(kW0, a22, t);
 }
 
-__device__ inline double sim_cell_fast(double mr, double rms, double srs, double md, double dms, double sds,
+// sr, sd: signed roots of the reference and degraded variances.
+__device__ inline double sim_cell_fast(double mr, double rms, double sr, double md, double dms, double sd,
                                        double crd) {
     const double mrd = mr * md;
     const double srd = crd - mrd;
-    const double prod = srs * sds;
-    const double sden = prod < 0.0 ? kC3 : sqrt(prod) + kC3;
+    const double q = sr * sd;
+    const double sden = q < 0.0 ? kC3 : fabs(q) + kC3;
     return (__fma_rn(2.0, mrd, kC1) * (srd + kC3)) / ((rms + dms + kC1) * sden);
 }
 
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(kThreads) table_kernel(const TableTask *__rest
                 const double cdsq = taps<kFast>(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12,
                                                 d20 * d20, d21 * d21, d22 * d22);
                 dms = md * md;
-                sds = cdsq - dms;
+                sds = kFast ? signed_root(cdsq - dms) : cdsq - dms;
             } else {
                 const int64_t pi = (int64_t)r * w + off + c;
                 md = mu[pi];

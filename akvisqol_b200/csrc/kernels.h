@@ -15,6 +15,7 @@ struct PlaneJob {
     const double *spec;  // prepared degraded spectrogram, nb x nf
     int32_t nf, width;
     double *pad, *mu, *dms, *sds;  // nb x width each
+    int32_t roots;  // fast forms: sds holds the signed square root of the variance
 };
 
 // Reference-patch terms: spec columns [col, col+P) of a prepared
@@ -23,6 +24,7 @@ struct RefTermsJob {
     const double *spec;
     int32_t nf, col;
     double *out;
+    int32_t roots;  // fast forms: the variance term holds its signed square root
 };
 
 // NSIM table block: offsets [off0, min(off0+127, hi)] of one patch.
@@ -129,7 +131,9 @@ int gammatone_fast_frames_per_cta();
 void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, FastBandCoeffs *out);
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
                            int nb, const double *d_hann, int window, int hop, cudaStream_t s);
-// f64 FMA form: tiles of gammatone_frames_per_cta(nb) frames, as the exact kernel.
+// f64 FMA form: two frames per thread; tiles of frames_per_cta frames, one
+// of gammatone_f64fma_frames_candidates(nb) (the first is the default).
+std::vector<int> gammatone_f64fma_frames_candidates(int nb);
 void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
                              int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s);
 

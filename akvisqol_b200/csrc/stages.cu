@@ -162,12 +162,13 @@ int visqol_b200_nsim_table(const double *ref_spec, size_t nf_ref, const double *
             terms(np * 4 * nb * patch), sims(np * nf_deg);
         VQB_CUDA(cudaMemsetAsync(sims.p, 0, std::max<size_t>(1, np * nf_deg) * sizeof(double), e.stream()));
         const size_t pl = nb * width;
-        vqb::PlaneJob pj{ds.p, (int32_t)nf_deg, (int32_t)width, plane.p, plane.p + pl, plane.p + 2 * pl, plane.p + 3 * pl};
+        vqb::PlaneJob pj{ds.p, (int32_t)nf_deg, (int32_t)width, plane.p, plane.p + pl, plane.p + 2 * pl, plane.p + 3 * pl,
+                         0};
         std::vector<vqb::RefTermsJob> tj;
         std::vector<vqb::TableTask> tasks;
         for (size_t p = 0; p < np; ++p) {
             double *t = terms.p + p * 4 * nb * patch;
-            tj.push_back(vqb::RefTermsJob{rs.p, (int32_t)nf_ref, (int32_t)ref_idx[p], t});
+            tj.push_back(vqb::RefTermsJob{rs.p, (int32_t)nf_ref, (int32_t)ref_idx[p], t, 0});
             for (int64_t o = lo[p]; o <= hi[p]; o += vqb::table_offsets_per_cta())
                 tasks.push_back(vqb::TableTask{t, pj.pad, pj.mu, pj.dms, pj.sds, (int32_t)width, (int32_t)o,
                                                (int32_t)hi[p], sims.p + p * nf_deg});

@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--batch", type=int, default=64)
+    p.add_argument("--batch", type=int, default=128)
     p.add_argument("--seconds", type=float, default=10.0)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fast", choices=["fast", "balanced", "exact"])
