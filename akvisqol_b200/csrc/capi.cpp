@@ -28,10 +28,12 @@
 using vqb::Error;
 
 // A context owns one or more lanes: engines with their own streams and
-// memory on the same GPU (VISQOL_GPU_LANES, default 2, as the reference's
-// GPU engine, src/gpu/engine.zig:551-591). A batch is split across the
+// memory on the same GPU (VISQOL_GPU_LANES, default 4; the reference's GPU
+// engine runs two, src/gpu/engine.zig:551-591). A batch is split across the
 // lanes by signal length and the lanes run concurrently from host threads,
-// so one lane's serial phases and host planning overlap another's kernels.
+// so one lane's serial phases, host planning and uploads overlap another's
+// kernels. On one B200, 4 lanes score a 128-pair batch of 10 s 48 kHz host
+// signals ~5% faster than 2 (the device-resident rate is the same).
 // References prepared once for many degraded signals (visqol_b200_prepare).
 struct visqol_b200_prepared {
     int device = 0;
@@ -146,8 +148,17 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
                const vqb::PreparedRef *const *prepared = nullptr) {
     const size_t L = std::min(c->lanes.size(), std::max<size_t>(1, n));
     res.assign(n, vqb::PairOutcome{});
+    // Host inputs: each lane overlaps its uploads with its scoring.
+    const bool streamed = !device_inputs && vqb::env_streamed_uploads();
+    auto measure = [&](vqb::Engine &e, size_t m, const double *const *r, const size_t *rl, const double *const *d,
+                       const size_t *dl, std::vector<vqb::PairOutcome> &o, const vqb::PreparedRef *const *pr) {
+        if (streamed)
+            e.measure_batch_streamed(m, r, rl, d, dl, sample_rate, o, pr);
+        else
+            e.measure_batch(m, r, rl, d, dl, sample_rate, device_inputs, o, pr);
+    };
     if (L <= 1) {
-        c->lanes[0]->measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res, prepared);
+        measure(*c->lanes[0], n, refs, ref_lens, degs, deg_lens, res, prepared);
         c->timing = c->lanes[0]->last_timing();
         return;
     }
@@ -175,8 +186,8 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
                 r[k] = refs[ix[k]], d[k] = degs[ix[k]], rl[k] = ref_lens[ix[k]], dl[k] = deg_lens[ix[k]];
                 if (prepared) pr[k] = prepared[ix[k]];
             }
-            c->lanes[l]->measure_batch(ix.size(), r.data(), rl.data(), d.data(), dl.data(), sample_rate, device_inputs,
-                                       lane_out[l], prepared ? pr.data() : nullptr);
+            measure(*c->lanes[l], ix.size(), r.data(), rl.data(), d.data(), dl.data(), lane_out[l],
+                    prepared ? pr.data() : nullptr);
         } catch (...) {
             errs[l] = std::current_exception();
         }
@@ -302,6 +313,11 @@ int vqb::context_device(int *device, std::string *message) {
     return VISQOL_OK;
 }
 
+bool vqb::env_streamed_uploads() {
+    const char *env = std::getenv("VISQOL_STREAMED_UPLOADS");
+    return !(env && env[0] == '0');
+}
+
 int vqb::env_lanes(int fallback) {
     int lanes = fallback;
     if (const char *env = std::getenv("VISQOL_GPU_LANES")) lanes = std::atoi(env);
@@ -350,7 +366,7 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
         if (int rc = vqb::engine_options(o, &c->opt, &c->svr, &lattice, &msg)) return fail(rc, msg);
         int dev = 0;
         if (int rc = vqb::context_device(&dev, &msg)) return fail(rc, msg);
-        const int lanes = vqb::env_lanes(2);
+        const int lanes = vqb::env_lanes(4);
         for (int l = 0; l < lanes; ++l)
             c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr, lattice));
     } catch (const Error &e) {

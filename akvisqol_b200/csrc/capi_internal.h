@@ -27,4 +27,8 @@ int context_device(int *device, std::string *message);
 // Number of lanes asked for by VISQOL_GPU_LANES (1-8, default fallback).
 int env_lanes(int fallback);
 
+// Whether host-input batches overlap their uploads with scoring
+// (Engine::measure_batch_streamed); VISQOL_STREAMED_UPLOADS=0 turns it off.
+bool env_streamed_uploads();
+
 }  // namespace vqb

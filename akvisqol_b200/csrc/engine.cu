@@ -25,6 +25,7 @@
 #include <tuple>
 #include <mutex>
 #include <functional>
+#include <future>
 
 #include "engine.h"
 
@@ -50,6 +51,22 @@ namespace {
 constexpr size_t kAlign = 256;
 constexpr size_t kChunk = size_t(256) << 20;
 inline size_t round_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+// Zero-fill on the compute stream as a kernel (no copy-engine work, so it
+// cannot queue behind a signal upload that another stream has in flight).
+__global__ void __launch_bounds__(256) zero_kernel(uint4 *__restrict__ dst, size_t n16) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// dst: an arena block (256-byte aligned and rounded, so whole 16-byte
+// words may be written).
+void launch_zero(void *dst, size_t bytes, cudaStream_t s) {
+    const size_t n16 = (bytes + 15) / 16;
+    const size_t blocks = std::min<size_t>((n16 + 255) / 256, 256);
+    zero_kernel<<<(unsigned)std::max<size_t>(1, blocks), 256, 0, s>>>(static_cast<uint4 *>(dst), n16);
+    launch_counter() += 1;
+}
 }  // namespace
 
 Arena::~Arena() {
@@ -128,6 +145,9 @@ Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> 
     VQB_CUDA(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, lo_prio));
     VQB_CUDA(cudaEventCreateWithFlags(&ev_inputs_, cudaEventDisableTiming));
     VQB_CUDA(cudaEventCreateWithFlags(&ev_ref_done_, cudaEventDisableTiming));
+    VQB_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+    for (auto &e : ev_up_) VQB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    VQB_CUDA(cudaEventCreateWithFlags(&ev_piece_, cudaEventDisableTiming));
     events_.resize(8);
     for (auto &e : events_) VQB_CUDA(cudaEventCreate(&e));
     for (auto &e : gt_events_) VQB_CUDA(cudaEventCreate(&e));
@@ -141,6 +161,12 @@ Engine::~Engine() {
     cudaSetDevice(device_);
     if (stream_) cudaStreamSynchronize(stream_);
     if (side_) cudaStreamSynchronize(side_);
+    if (copy_) cudaStreamSynchronize(copy_);
+    for (auto e : ev_up_)
+        if (e) cudaEventDestroy(e);
+    if (ev_piece_) cudaEventDestroy(ev_piece_);
+    for (auto p : slot_) cudaFree(p);
+    if (copy_) cudaStreamDestroy(copy_);
     if (ev_inputs_) cudaEventDestroy(ev_inputs_);
     if (ev_ref_done_) cudaEventDestroy(ev_ref_done_);
     if (side_) cudaStreamDestroy(side_);
@@ -608,7 +634,8 @@ struct PairState {
 
 void Engine::measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                            const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
-                           std::vector<PairOutcome> &out, const PreparedRef *const *prepared) {
+                           std::vector<PairOutcome> &out, const PreparedRef *const *prepared,
+                           const double *const *host_refs) {
     out.assign(n, PairOutcome{});
     timing_ = Timing{};
     if (n == 0) return;
@@ -644,6 +671,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         if (device_inputs) {
             s.ref = s.prep ? s.prep->d_sig : refs[i];
             s.deg = degs[i];
+            if (host_refs && !s.prep) s.h_ref = host_refs[i];
         } else {
             double *d = arena_.alloc_n<double>(s.dl);
             if (s.dl) VQB_CUDA(cudaMemcpyAsync(d, degs[i], s.dl * sizeof(double), cudaMemcpyHostToDevice, stream_));
@@ -663,6 +691,12 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         s.stats = arena_.alloc_n<double>(10);
     }
 
+    auto launch_prep_jobs = [&](const std::vector<PrepJob> &jobs) {
+        int max_frames = 0;
+        for (const PrepJob &j : jobs) max_frames = std::max({max_frames, (int)j.nfr, (int)j.nfd});
+        double *scratch = arena_.alloc_n<double>(prep_scratch_count((int)jobs.size(), max_frames));
+        launch_prep(upload(jobs), (int)jobs.size(), nbi, max_frames, scratch, stream_);
+    };
     auto run_gammatone = [&](const std::vector<SpecJob> &jobs, cudaStream_t st) {
         if (jobs.empty()) return;
         const size_t slot = 2 * timing_.gammatone_launches;
@@ -694,7 +728,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
 
     // ---- 1: global lag and SPL energies --------------------------------
     int64_t *d_lags = arena_.alloc_n<int64_t>(n);
-    VQB_CUDA(cudaMemsetAsync(d_lags, 0, n * sizeof(int64_t), stream_));
+    launch_zero(d_lags, n * sizeof(int64_t), stream_);
     {
         std::vector<SumJob> sums;
         std::vector<LagJob> lag_jobs;
@@ -757,6 +791,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     std::vector<RefTermsJob> term_jobs;
     std::vector<TableTask> table_rows;  // one per patch: offsets [off0, hi]
     std::vector<DpJob> dp_jobs;
+    std::vector<int64_t> all_lohi;  // per DP job: its patches' lo, then hi
+    std::vector<size_t> lohi_at;
     std::vector<StatsJob> stat_jobs;
     int max_width = 0;
     for (size_t i = 0; i < n; ++i) {
@@ -827,13 +863,9 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         prep_jobs.push_back(PrepJob{s.ref_raw, s.deg_raw, s.ref_prep, s.deg_prep, (int32_t)s.nf_ref, (int32_t)s.nf_deg});
         plane_jobs.push_back(PlaneJob{s.deg_prep, (int32_t)s.nf_deg, (int32_t)s.width, s.pad, s.mu, s.dms, s.sds,
                                       opt_.form != kFormExact ? 1 : 0});
-        int64_t *d_lo = nullptr;
-        {
-            std::vector<int64_t> lohi(2 * np);
-            std::copy(s.search.lo.begin(), s.search.lo.end(), lohi.begin());
-            std::copy(s.search.hi.begin(), s.search.hi.end(), lohi.begin() + np);
-            d_lo = upload(lohi);
-        }
+        lohi_at.push_back(all_lohi.size());
+        all_lohi.insert(all_lohi.end(), s.search.lo.begin(), s.search.lo.end());
+        all_lohi.insert(all_lohi.end(), s.search.hi.begin(), s.search.hi.end());
         for (size_t p = 0; p < np; ++p) {
             double *terms = s.terms + p * 4 * NB * P;
             term_jobs.push_back(RefTermsJob{s.ref_prep, (int32_t)s.nf_ref, (int32_t)s.idx[p], terms,
@@ -847,7 +879,15 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                                          s.valid + p, ms, ms + NB, ms + 2 * NB, ms + 3 * NB});
             s.trace.n_cells += NB * P;
         }
-        dp_jobs.push_back(DpJob{s.sims, d_lo, d_lo + np, (int32_t)np, (int64_t)s.nf_deg, s.dp, s.bt, s.offs, s.valid});
+        dp_jobs.push_back(DpJob{s.sims, nullptr, nullptr, (int32_t)np, (int64_t)s.nf_deg, s.dp, s.bt, s.offs, s.valid});
+    }
+    // every pair's search windows in one upload
+    if (!dp_jobs.empty()) {
+        const int64_t *d_lohi = upload(all_lohi);
+        for (size_t k = 0; k < dp_jobs.size(); ++k) {
+            dp_jobs[k].lo = d_lohi + lohi_at[k];
+            dp_jobs[k].hi = dp_jobs[k].lo + dp_jobs[k].np;
+        }
     }
 
     // ---- 3: spectrograms, prep, NSIM table, DP, match statistics ----------
@@ -856,7 +896,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     run_gammatone(spec_jobs, stream_);
     record(events_[3]);
     VQB_CUDA(cudaStreamWaitEvent(stream_, ev_ref_done_, 0));
-    if (!prep_jobs.empty()) launch_prep(upload(prep_jobs), (int)prep_jobs.size(), nbi, stream_);
+    if (!prep_jobs.empty()) launch_prep_jobs(prep_jobs);
     record(events_[4]);
     if (!plane_jobs.empty()) launch_plane(upload(plane_jobs), (int)plane_jobs.size(), nbi, max_width, stream_);
     if (!term_jobs.empty()) launch_ref_terms(upload(term_jobs), (int)term_jobs.size(), nbi, (int)P, stream_);
@@ -1028,7 +1068,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         // ---- 7: realigned spectrograms and statistics ------------------------
         if (!copies.empty()) launch_copy_frames(upload(copies), (int)copies.size(), nbi, max_cols, stream_);
         run_gammatone(rjobs, stream_);
-        if (!rprep.empty()) launch_prep(upload(rprep), (int)rprep.size(), nbi, stream_);
+        if (!rprep.empty()) launch_prep_jobs(rprep);
         if (!rstats.empty()) launch_stats(upload(rstats), (int)rstats.size(), nbi, stream_);
         std::vector<double *> h_rst;
         for (auto &s : ps) {
@@ -1115,6 +1155,138 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     timing_.prep_ms = elapsed(events_[3], events_[4]);
     timing_.nsim_ms = elapsed(events_[4], events_[5]);
     timing_.realign_ms = n_slices ? elapsed(events_[5], events_[6]) : 0.0;
+}
+
+void Engine::measure_batch_streamed(size_t n, const double *const *refs, const size_t *ref_lens,
+                                    const double *const *degs, const size_t *deg_lens, uint32_t sample_rate,
+                                    std::vector<PairOutcome> &out, const PreparedRef *const *prepared) {
+    // Bytes each pair uploads, each signal at a 256-byte boundary of its slot.
+    auto up = [](size_t len) { return (len * sizeof(double) + 255) & ~size_t(255); };
+    auto ref_up = [&](size_t i) {
+        return (prepared && prepared[i]) || !refs[i] ? size_t(0) : up(ref_lens[i]);
+    };
+    auto deg_up = [&](size_t i) { return degs[i] ? up(deg_lens[i]) : size_t(0); };
+    size_t total = 0;
+    for (size_t i = 0; i < n; ++i) total += ref_up(i) + deg_up(i);
+    // Below ~64 MiB the exposed first upload and the per-chunk host work
+    // outweigh the overlap (VISQOL_STREAMED_MIN_BYTES overrides the bound).
+    size_t min_bytes = size_t(64) << 20;
+    if (const char *env = std::getenv("VISQOL_STREAMED_MIN_BYTES")) min_bytes = (size_t)std::strtoull(env, nullptr, 10);
+    if (n < 2 || total < min_bytes) {
+        measure_batch(n, refs, ref_lens, degs, deg_lens, sample_rate, false, out, prepared);
+        return;
+    }
+    // Chunks of 1/16, 1/8, 1/4 ... of the bytes (a small first chunk keeps
+    // the exposed first upload short; each later upload has the previous,
+    // half-as-large chunk's scoring to hide behind); a tail smaller than
+    // half the next target joins the last chunk.
+    std::vector<size_t> bounds{0};
+    {
+        size_t target = std::max<size_t>(1, total / 16), acc = 0, left = total;
+        for (size_t i = 0; i < n; ++i) {
+            const size_t b = ref_up(i) + deg_up(i);
+            acc += b;
+            left -= b;
+            if (acc >= target && i + 1 < n) {
+                if (left < target) continue;  // the rest is small: keep it in this chunk
+                bounds.push_back(i + 1);
+                acc = 0;
+                target *= 2;
+            }
+        }
+        bounds.push_back(n);
+    }
+    const size_t K = bounds.size() - 1;
+    std::vector<size_t> chunk_bytes(K, 0);
+    for (size_t k = 0; k < K; ++k)
+        for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) chunk_bytes[k] += ref_up(i) + deg_up(i);
+    VQB_CUDA(cudaSetDevice(device_));
+    for (int sl = 0; sl < 2; ++sl) {
+        size_t need = 0;
+        for (size_t k = sl; k < K; k += 2) need = std::max(need, chunk_bytes[k]);
+        if (need > slot_bytes_[sl]) {
+            VQB_CUDA(cudaStreamSynchronize(copy_));
+            if (slot_[sl]) VQB_CUDA(cudaFree(slot_[sl]));
+            slot_[sl] = nullptr;
+            slot_bytes_[sl] = 0;
+            VQB_CUDA(cudaMalloc(&slot_[sl], need));
+            slot_bytes_[sl] = need;
+        }
+    }
+    // Device views of chunk k's signals in slot k & 1 (NULL where the pair
+    // has nothing to upload, so measure_batch reports it as the host path does).
+    std::vector<const double *> d_ref(n, nullptr), d_deg(n, nullptr);
+    for (size_t k = 0; k < K; ++k) {
+        char *base = reinterpret_cast<char *>(slot_[k & 1]);
+        size_t off = 0;
+        for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) {
+            if (ref_up(i)) d_ref[i] = reinterpret_cast<const double *>(base + off), off += ref_up(i);
+            if (deg_up(i)) d_deg[i] = reinterpret_cast<const double *>(base + off), off += deg_up(i);
+        }
+    }
+    // A chunk goes up one copy at a time (each signal, in pieces of at most
+    // 64 MiB), the next issued when the previous has landed: the scoring
+    // streams' own small uploads (job arrays) share the copy engines, and
+    // behind a whole queued chunk they would stall their kernels until the
+    // chunk had landed. Measured on the 10 s 48 kHz batch, one copy in flight
+    // beat finer pieces with more in flight and the whole chunk queued at
+    // once.
+    constexpr size_t kPiece = size_t(64) << 20;
+    auto upload_chunk = [&](size_t k) {
+        VQB_CUDA(cudaSetDevice(device_));
+        size_t pieces = 0;
+        auto copy = [&](const double *dst, const double *src, size_t len) {
+            const char *s8 = reinterpret_cast<const char *>(src);
+            char *d8 = reinterpret_cast<char *>(const_cast<double *>(dst));
+            const size_t bytes = len * sizeof(double);
+            for (size_t o = 0; o < bytes; o += kPiece, ++pieces) {
+                if (pieces) VQB_CUDA(cudaEventSynchronize(ev_piece_));
+                VQB_CUDA(cudaMemcpyAsync(d8 + o, s8 + o, std::min(kPiece, bytes - o), cudaMemcpyHostToDevice, copy_));
+                VQB_CUDA(cudaEventRecord(ev_piece_, copy_));
+            }
+        };
+        for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) {
+            if (d_ref[i] && ref_lens[i]) copy(d_ref[i], refs[i], ref_lens[i]);
+            if (d_deg[i] && deg_lens[i]) copy(d_deg[i], degs[i], deg_lens[i]);
+        }
+        VQB_CUDA(cudaEventRecord(ev_up_[k & 1], copy_));
+    };
+    out.assign(n, PairOutcome{});
+    Timing sum{};
+    uint64_t h2d = 0;
+    for (size_t i = 0; i < n; ++i)
+        h2d += (d_ref[i] ? ref_lens[i] : 0) * sizeof(double) + (d_deg[i] ? deg_lens[i] : 0) * sizeof(double);
+    std::vector<PairOutcome> part;
+    upload_chunk(0);
+    for (size_t k = 0; k < K; ++k) {
+        // Chunk k+1 goes into the other slot, last read by chunk k-1, whose
+        // scoring has returned (measure_batch ends with its stream drained).
+        std::future<void> next;
+        if (k + 1 < K) next = std::async(std::launch::async, upload_chunk, k + 1);
+        VQB_CUDA(cudaStreamWaitEvent(stream_, ev_up_[k & 1], 0));
+        const size_t b0 = bounds[k], m = bounds[k + 1] - b0;
+        measure_batch(m, d_ref.data() + b0, ref_lens + b0, d_deg.data() + b0, deg_lens + b0, sample_rate, true,
+                      part, prepared ? prepared + b0 : nullptr, refs + b0);
+        if (next.valid()) next.get();
+        for (size_t j = 0; j < m; ++j) out[b0 + j] = std::move(part[j]);
+        const Timing &t = timing_;
+        sum.total_ms += t.total_ms;
+        sum.lag_ms += t.lag_ms;
+        sum.spectrogram_ms += t.spectrogram_ms;
+        sum.prep_ms += t.prep_ms;
+        sum.nsim_ms += t.nsim_ms;
+        sum.realign_ms += t.realign_ms;
+        sum.gammatone_kernel_ms += t.gammatone_kernel_ms;
+        sum.gammatone_launches += t.gammatone_launches;
+        sum.gammatone_rms += t.gammatone_rms;
+        sum.gammatone_window = std::max(sum.gammatone_window, t.gammatone_window);
+        sum.kernel_launches += t.kernel_launches;
+        sum.h2d_bytes += t.h2d_bytes;
+        sum.d2h_bytes += t.d2h_bytes;
+        sum.host_syncs += t.host_syncs;
+    }
+    sum.h2d_bytes += h2d;
+    timing_ = sum;
 }
 
 }  // namespace vqb

@@ -122,9 +122,22 @@ public:
     // device_inputs. Per-pair failures land in out[i].code.
     // With prepared non-NULL, pair i whose prepared[i] is set takes its
     // reference from there (refs[i] and ref_lens[i] are ignored).
+    // host_refs (device inputs only, may be NULL): host copies of the
+    // references, read by the speech-mode VAD instead of a read-back.
     void measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                        const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
-                       std::vector<PairOutcome> &out, const PreparedRef *const *prepared = nullptr);
+                       std::vector<PairOutcome> &out, const PreparedRef *const *prepared = nullptr,
+                       const double *const *host_refs = nullptr);
+    // Host inputs scored in consecutive chunks of growing size: chunk k+1's
+    // signals are copied to the device on a copy stream (from a helper
+    // thread, so pageable sources do not block scoring) while chunk k is
+    // scored, so the host-to-device transfer overlaps the GPU work instead of
+    // preceding it. Results are identical to measure_batch with host inputs
+    // (every pair's result depends only on its own signals). Small batches
+    // take the direct path.
+    void measure_batch_streamed(size_t n, const double *const *refs, const size_t *ref_lens,
+                                const double *const *degs, const size_t *deg_lens, uint32_t sample_rate,
+                                std::vector<PairOutcome> &out, const PreparedRef *const *prepared = nullptr);
     // Reference-side work of n references in this engine's form and mode.
     void prepare(size_t n, const double *const *refs, const size_t *ref_lens, uint32_t sample_rate,
                  bool device_inputs, std::vector<std::unique_ptr<PreparedRef>> &out);
@@ -199,6 +212,13 @@ private:
     cudaEvent_t ev_inputs_ = nullptr, ev_ref_done_ = nullptr;
     cudaEvent_t gt_events_[6] = {};  // begin/end of up to three gammatone launches
     Timing timing_;
+    // measure_batch_streamed: copy stream, two upload slots (grow-only
+    // device buffers) and the events that mark each slot's upload done.
+    cudaStream_t copy_ = nullptr;
+    cudaEvent_t ev_up_[2] = {};
+    cudaEvent_t ev_piece_ = nullptr;  // the upload copy in flight
+    double *slot_[2] = {};
+    size_t slot_bytes_[2] = {};
 };
 
 // The autotuner's choices so far: (device, kernel, variant a, variant b,

@@ -13,24 +13,31 @@
 // f32 form (gammatone_fast_kernel) splits the cascade across the two
 // arithmetic pipes of an SM:
 //
-// * stage 1 runs in f64 with FMA on the FP64 pipe. It sees the raw windowed
+// * stages 1 and 2 run in f64 with FMA on the FP64 pipe, direct form I with
+//   unit-leading numerators (3 FMAs a stage). Stage 1 sees the raw windowed
 //   signal, whose out-of-band content is far larger than the band's output;
 //   f32 state there would carry rounding of that content into the result.
-// * stages 2-4 run in f32 on the FP32 pipe, two frames per thread as packed
-//   f32x2 FMAs. Their numerators are normalised to 1 + beta z^-1 with the
-//   gains (a0^3) applied to the final RMS in f64, and their pole
-//   coefficients are carried as hi + lo f32 pairs: rounding the poles to a
-//   single f32 shifts the upper bands' responses enough to move MOS by
-//   ~6e-7. Bands whose centre frequencies are low (poles near z = 1) use the
-//   direct form I recurrence, the rest the transposed direct form II; each
-//   kept the smaller error in a sweep over both.
+// * stages 3 and 4 run in f32 on the FP32 pipe, two frames per thread as
+//   packed f32x2 FMAs. Their pole coefficients are carried as hi + lo f32
+//   pairs: rounding the poles to a single f32 shifts the upper bands'
+//   responses enough to move MOS by ~6e-7. Bands whose centre frequencies
+//   are low (poles near z = 1) use the direct form I recurrence, the rest
+//   the transposed direct form II; each kept the smaller error in a sweep
+//   over both. All numerator gains go into one f64 factor on the RMS.
 // * the squared outputs are summed in f32 over runs of 16 samples and the
 //   runs are added in f64.
 //
-// A warp holds 8 bands x 4 frame pairs: lanes of a frame pair load the same
-// sample (4 distinct addresses per load), the Hann value is warp-uniform,
-// and every band of a warp takes the same form (the host groups bands by 8).
-// A CTA holds ceil(nb/8) band groups x 2 frame blocks of 8 frames.
+// Per frame-sample that is 6 FP64 FMAs (16 lanes per SM sub-partition) and
+// 11-13 FP32 FMAs (32 lanes), which keeps both pipes about equally busy.
+// The CTA's 16 frames are Hann-windowed once per 64-sample tile into shared
+// memory (double-buffered; the next tile's samples are loaded into registers
+// while the current one is filtered), so a thread reads its two frames'
+// windowed samples with one 16-byte load per step.
+//
+// A warp holds 8 bands x 4 frame pairs: lanes of a frame pair read the same
+// shared-memory word (a broadcast), and every band of a warp takes the same
+// form (the host groups bands by 8). A CTA holds ceil(nb/8) band groups x 2
+// frame blocks of 8 frames.
 #include "device.cuh"
 #include "kernels.h"
 
@@ -45,9 +52,20 @@ struct Tile {
 
 constexpr int kFramesPerBlock = 8;   // frames per warp (4 lanes rows x 2)
 constexpr int kBlocksPerCta = 2;
+constexpr int kCtaFrames = kFramesPerBlock * kBlocksPerCta;
 constexpr int kRun = 16;             // f32 partial-sum run length
+constexpr int kTileS = 64;           // samples per shared-memory tile
+constexpr int kRowPad = kCtaFrames + 2;  // doubles per tile row (2-way write conflicts, 16-byte reads)
 
 __device__ inline float2 f2(float v) { return make_float2(v, v); }
+
+// 8-byte asynchronous global-to-shared copy; bytes = 0 writes zeros.
+__device__ inline void cp_async8(double *dst, const double *src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct F32Stage {
     float2 a, b, c;  // DF2T: c0, c1 (c unused); DF-I: y1, y2, previous input
@@ -77,6 +95,140 @@ __device__ inline float2 stage32(float2 v, F32Stage &s, float2 beta, float2 np1h
     return y;
 }
 
+// Stages 1 and 2 of one frame in f64, direct form I with unit-leading
+// numerators: y = x + b0 x[-1] - d2 y[-2] - d1 y[-1], then the same on y.
+struct F64Pair {
+    double x1 = 0.0, y1 = 0.0, y2 = 0.0, z1 = 0.0, z2 = 0.0;
+    __device__ inline double step(double x, double b0, double b1, double nd1, double nd2) {
+        const double y = __fma_rn(nd1, y1, __fma_rn(nd2, y2, __fma_rn(b0, x1, x)));
+        const double z = __fma_rn(nd1, z1, __fma_rn(nd2, z2, __fma_rn(b1, y1, y)));
+        x1 = x;
+        y2 = y1;
+        y1 = y;
+        z2 = z1;
+        z1 = z;
+        return z;
+    }
+};
+
+template <bool kDirectI>
+__device__ inline void filter_tile(const double (*__restrict__ wx)[kRowPad], int q, int count,
+                                   const FastBandCoeffs &k, F64Pair &A, F64Pair &B, F32Stage (&st)[2],
+                                   double &acc_a, double &acc_b) {
+    const double b0 = k.beta64[0], b1 = k.beta64[1], nd1 = -k.d1, nd2 = -k.d2;
+    const float2 c3 = f2(k.beta[0]), c4 = f2(k.beta[1]);
+    const float2 np1h = f2(-k.p1h), np1l = f2(-k.p1l), np2h = f2(-k.p2h), np2l = f2(-k.p2l);
+    auto step = [&](int i, float2 &part) {
+        const double2 w = *reinterpret_cast<const double2 *>(&wx[i][q]);
+        const double za = A.step(w.x, b0, b1, nd1, nd2);
+        const double zb = B.step(w.y, b0, b1, nd1, nd2);
+        float2 v = make_float2(__double2float_rn(za), __double2float_rn(zb));
+        v = stage32<kDirectI>(v, st[0], c3, np1h, np1l, np2h, np2l);
+        v = stage32<kDirectI>(v, st[1], c4, np1h, np1l, np2h, np2l);
+        part = __ffma2_rn(v, v, part);
+    };
+    if (count == kTileS) {
+#pragma unroll 1
+        for (int r = 0; r < kTileS / kRun; ++r) {
+            float2 part = f2(0.f);
+#pragma unroll 4
+            for (int j = 0; j < kRun; ++j) step(r * kRun + j, part);
+            acc_a += (double)part.x;
+            acc_b += (double)part.y;
+        }
+    } else {
+        float2 part = f2(0.f);
+        for (int i = 0; i < count; ++i) step(i, part);
+        acc_a += (double)part.x;
+        acc_b += (double)part.y;
+    }
+}
+
+// kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 768 / kThreads) gammatone_fast_kernel(
+    const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, const FastBandCoeffs *__restrict__ coeffs,
+    int nb, const double *__restrict__ hann, int window, int hop) {
+    __shared__ __align__(16) double raw[2][kCtaFrames][kTileS];  // signal samples, frame-major
+    __shared__ __align__(16) double wx[2][kTileS][kRowPad];      // windowed, sample-major
+    const Tile tile = tiles[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int groups = (nb + 7) >> 3;
+    const int g = warp % groups, fblock = warp / groups;
+    const int band_raw = g * 8 + (lane & 7);
+    const int band = band_raw < nb ? band_raw : nb - 1;  // idle lanes filter a real band, never write
+    const int q = fblock * kFramesPerBlock + 2 * (lane >> 3);
+    const SpecJob job = jobs[tile.job];
+    const VSig sig = job.sig;
+    const int64_t f = (int64_t)tile.frame0 + q;
+    const FastBandCoeffs k = coeffs[band];
+
+    // Tiles of kTileS samples of the CTA's frames: entry e = (frame c =
+    // e / kTileS, sample i = e % kTileS), so consecutive threads copy
+    // consecutive samples of a frame. Samples outside the signal's stored
+    // range or past the window are zero-filled by the copy itself.
+    constexpr int kFills = (kCtaFrames * kTileS + kThreads - 1) / kThreads;
+    auto fetch = [&](int i0, int buf) {
+#pragma unroll
+        for (int m = 0; m < kFills; ++m) {
+            const int e = threadIdx.x + m * kThreads;
+            if (e < kCtaFrames * kTileS) {
+                const int c = e / kTileS, i = e - c * kTileS;
+                const int64_t j = ((int64_t)tile.frame0 + c) * hop + i0 + i - sig.head;
+                const bool in = i0 + i < window && (uint64_t)j < (uint64_t)sig.avail;
+                cp_async8(&raw[buf][c][i], in ? sig.base + j : sig.base, in ? 8 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    auto windowed = [&](int i0, int buf) {
+#pragma unroll
+        for (int m = 0; m < kFills; ++m) {
+            const int e = threadIdx.x + m * kThreads;
+            if (e < kCtaFrames * kTileS) {
+                const int c = e / kTileS, i = e - c * kTileS;
+                wx[buf][i][c] = i0 + i < window ? raw[buf][c][i] * __ldg(hann + i0 + i) : 0.0;
+            }
+        }
+    };
+    fetch(0, 0);
+    cp_async_wait_all();
+    __syncthreads();
+    windowed(0, 0);
+    __syncthreads();
+
+    F64Pair A, B;
+    F32Stage st[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) st[s] = F32Stage{f2(0.f), f2(0.f), f2(0.f)};
+    double acc_a = 0.0, acc_b = 0.0;
+    // Tile t+1's copies are in flight while tile t is filtered; its windowing
+    // waits for them (and for every thread to be done reading the buffers it
+    // overwrites, which were tile t-1's).
+    int buf = 0;
+    for (int i0 = 0; i0 < window; i0 += kTileS) {
+        const bool more = i0 + kTileS < window;
+        if (more) fetch(i0 + kTileS, buf ^ 1);
+        const int count = window - i0 < kTileS ? window - i0 : kTileS;
+        if (k.direct_i)
+            filter_tile<true>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
+        else
+            filter_tile<false>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
+        if (more) {
+            cp_async_wait_all();
+            __syncthreads();
+            windowed(i0 + kTileS, buf ^ 1);
+            __syncthreads();
+        }
+        buf ^= 1;
+    }
+    if (band_raw >= nb || f >= job.nf) return;
+    const double inv_n = 1.0 / (double)window;
+    double *out = job.out + (int64_t)band * job.nf;
+    out[f] = sqrt(acc_a * inv_n) * k.post64;
+    if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post64;
+}
+
 // Samples of a frame: straight loads when the whole window lies inside the
 // signal's stored samples (nearly every frame), else VSig's bounds-checked
 // view (zero padding at slice edges).
@@ -91,83 +243,6 @@ struct Checked {
 
 __device__ inline bool window_inside(const VSig &sig, int64_t k0, int64_t span) {
     return k0 - sig.head >= 0 && k0 + span - sig.head <= sig.avail;
-}
-
-template <bool kDirectI, class Load>
-__device__ void band_frames(const Load &sample, int64_t ka, int64_t kb, const FastBandCoeffs &k,
-                            const double *__restrict__ hann, int window, double &acc_a, double &acc_b) {
-    double c0a = 0.0, c1a = 0.0, c0b = 0.0, c1b = 0.0;
-    F32Stage st[3];
-#pragma unroll
-    for (int s = 0; s < 3; ++s) st[s] = F32Stage{f2(0.f), f2(0.f), f2(0.f)};
-    const float2 b0 = f2(k.beta[0]), b1 = f2(k.beta[1]), b2 = f2(k.beta[2]);
-    const float2 np1h = f2(-k.p1h), np1l = f2(-k.p1l), np2h = f2(-k.p2h), np2l = f2(-k.p2l);
-    const double n0 = k.n0, n1 = k.n1, nd1 = -k.d1, nd2 = -k.d2;
-    acc_a = 0.0;
-    acc_b = 0.0;
-    auto step = [&](int i, float2 &part) {
-        const double h = __ldg(hann + i);
-        const double xa = sample(ka + i) * h;
-        const double xb = sample(kb + i) * h;
-        const double fa = __fma_rn(n0, xa, c0a);
-        const double fb = __fma_rn(n0, xb, c0b);
-        c0a = __fma_rn(nd1, fa, __fma_rn(n1, xa, c1a));
-        c0b = __fma_rn(nd1, fb, __fma_rn(n1, xb, c1b));
-        c1a = nd2 * fa;
-        c1b = nd2 * fb;
-        float2 v = make_float2(__double2float_rn(fa), __double2float_rn(fb));
-        v = stage32<kDirectI>(v, st[0], b0, np1h, np1l, np2h, np2l);
-        v = stage32<kDirectI>(v, st[1], b1, np1h, np1l, np2h, np2l);
-        v = stage32<kDirectI>(v, st[2], b2, np1h, np1l, np2h, np2l);
-        part = __ffma2_rn(v, v, part);
-    };
-    const int runs = window / kRun;
-    for (int r = 0; r < runs; ++r) {
-        float2 part = f2(0.f);
-#pragma unroll
-        for (int j = 0; j < kRun; ++j) step(r * kRun + j, part);
-        acc_a += (double)part.x;
-        acc_b += (double)part.y;
-    }
-    float2 part = f2(0.f);
-    for (int i = runs * kRun; i < window; ++i) step(i, part);
-    acc_a += (double)part.x;
-    acc_b += (double)part.y;
-}
-
-__global__ void __launch_bounds__(256) gammatone_fast_kernel(const SpecJob *__restrict__ jobs,
-                                                             const Tile *__restrict__ tiles,
-                                                             const FastBandCoeffs *__restrict__ coeffs, int nb,
-                                                             const double *__restrict__ hann, int window, int hop) {
-    const Tile tile = tiles[blockIdx.x];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int groups = (nb + 7) >> 3;
-    const int g = warp % groups, fblock = warp / groups;
-    const int band = g * 8 + (lane & 7);
-    const SpecJob job = jobs[tile.job];
-    const int64_t f = (int64_t)tile.frame0 + fblock * kFramesPerBlock + 2 * (lane >> 3);
-    if (band >= nb || f >= job.nf) return;
-    const FastBandCoeffs k = coeffs[band];
-    const int64_t ka = f * hop, kb = ka + hop;
-    double acc_a, acc_b;
-    const VSig &sig = job.sig;
-    if (window_inside(sig, ka, hop + window)) {
-        const Direct ld{sig.base - sig.head};
-        if (k.direct_i)
-            band_frames<true>(ld, ka, kb, k, hann, window, acc_a, acc_b);
-        else
-            band_frames<false>(ld, ka, kb, k, hann, window, acc_a, acc_b);
-    } else {
-        const Checked ld{sig};
-        if (k.direct_i)
-            band_frames<true>(ld, ka, kb, k, hann, window, acc_a, acc_b);
-        else
-            band_frames<false>(ld, ka, kb, k, hann, window, acc_a, acc_b);
-    }
-    const double inv_n = 1.0 / (double)window;
-    double *out = job.out + (int64_t)band * job.nf;
-    out[f] = sqrt(acc_a * inv_n) * k.post;
-    if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post;
 }
 
 // Two frames per thread (the second hop samples later): two independent
@@ -279,25 +354,21 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
         for (int b = g * 8; b <= hi; ++b) {
             const BandCoeffs &c = run[b];
             FastBandCoeffs &k = out[b];
-            k.n0 = c.s1n0;
-            k.n1 = c.s1n1;
+            const double a0 = c.ca0;
             k.d1 = c.d1;
             k.d2 = c.d2;
-            const double a0 = c.ca0;
-            k.post = fabs(a0 * a0 * a0);
-            k.beta[0] = (float)(c.s2n1 / a0);
-            k.beta[1] = (float)(c.s3n1 / a0);
-            k.beta[2] = (float)(c.s4n1 / a0);
-            k.p1h = (float)c.d1;
-            k.p1l = (float)(c.d1 - (double)k.p1h);
-            k.p2h = (float)c.d2;
-            k.p2l = (float)(c.d2 - (double)k.p2h);
-            k.direct_i = direct_i;
             k.beta64[0] = c.s1n1 / c.s1n0;
             k.beta64[1] = c.s2n1 / a0;
             k.beta64[2] = c.s3n1 / a0;
             k.beta64[3] = c.s4n1 / a0;
             k.post64 = fabs(c.s1n0 * a0 * a0 * a0);
+            k.beta[0] = (float)k.beta64[2];
+            k.beta[1] = (float)k.beta64[3];
+            k.p1h = (float)c.d1;
+            k.p1l = (float)(c.d1 - (double)k.p1h);
+            k.p2h = (float)c.d2;
+            k.p2l = (float)(c.d2 - (double)k.p2h);
+            k.direct_i = direct_i;
         }
     }
 }
@@ -305,9 +376,15 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
                            int nb, const double *d_hann, int window, int hop, cudaStream_t s) {
     if (ntiles <= 0) return;
-    const int threads = ((nb + 7) / 8) * kBlocksPerCta * 32;
-    gammatone_fast_kernel<<<ntiles, threads, 0, s>>>(d_jobs, static_cast<const Tile *>(d_tiles), d_coeffs, nb,
-                                                    d_hann, window, hop);
+    const Tile *t = static_cast<const Tile *>(d_tiles);
+    if (nb > 24)
+        gammatone_fast_kernel<256><<<ntiles, 256, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
+    else if (nb > 16)
+        gammatone_fast_kernel<192><<<ntiles, 192, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
+    else if (nb > 8)
+        gammatone_fast_kernel<128><<<ntiles, 128, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
+    else
+        gammatone_fast_kernel<64><<<ntiles, 64, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
     launch_counter() += 1;
 }
 

@@ -45,6 +45,12 @@ __device__ inline double2 cross_term(double2 x, double2 zy) {
     return make_double2(0.25 * (sum.x * idc.x - sum.y * idc.y), 0.25 * (sum.x * idc.y + sum.y * idc.x));
 }
 
+// 16-byte asynchronous global-to-shared copy (both addresses 16-byte aligned).
+__device__ inline void cp_async16(double2 *dst, const double2 *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
 __host__ __device__ inline int64_t pow2_at_least(int64_t x) {
     int64_t n = 1;
     while (n < x) n <<= 1;
@@ -193,24 +199,30 @@ __device__ inline void column_stages(double2 *x, int G, int cols, int64_t c0, co
 
 // Pass 1: pack + DIF column stages. grid (n / (R*cols) ... = 4096/cols, jobs).
 template <bool RAW>
-__global__ void __launch_bounds__(kThreads) fwd_columns(const LagJob *__restrict__ jobs, int G,
+__global__ void __launch_bounds__(kThreads, 3) fwd_columns(const LagJob *__restrict__ jobs, int G,
                                                         const double2 *__restrict__ tcol) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
-    const int R = 1 << G, cols = kB >> G > 0 ? (kB >> G) : 1;
+    const int cols = kB >> G > 0 ? (kB >> G) : 1;
     const int64_t c0 = (int64_t)blockIdx.x * cols;
     EnvParams pa{}, pb{};
     if (!RAW) {
         pa = env_params(job.a, job.stats_a);
         pb = env_params(job.b, job.stats_b);
     }
-    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+    // R * cols = kB points, a fixed 16 per thread: four at a time keeps
+    // eight signal loads in flight within the three-CTA register budget.
+#pragma unroll 4
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
         const int t = e / cols, c = e - t * cols;
         sm[e] = packed<RAW>(job, pa, pb, (int64_t)t * kB + c0 + c);
     }
     __syncthreads();
     column_stages<false>(sm, G, cols, c0, tcol);
-    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+#pragma unroll 4
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
         const int t = e / cols, c = e - t * cols;
         job.z[(int64_t)t * kB + c0 + c] = sm[e];
     }
@@ -503,17 +515,23 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
                                                                int64_t *pk, int parts) {
     extern __shared__ double2 sm[];
     const LagJob job = jobs[blockIdx.y];
-    const int R = 1 << G, cols = kB >> G > 0 ? (kB >> G) : 1;
+    const int cols = kB >> G > 0 ? (kB >> G) : 1;
     const int64_t c0 = (int64_t)blockIdx.x * cols;
-    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+    // The tile arrives by asynchronous 16-byte copies: all 16 of a thread's
+    // loads in flight at once, none staged through registers.
+#pragma unroll
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
         const int t = e / cols, c = e - t * cols;
-        sm[e] = job.z[(int64_t)t * kB + c0 + c];
+        cp_async16(sm + e, job.z + (int64_t)t * kB + c0 + c);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
     column_stages<true>(sm, G, cols, c0, tcol);
     const int64_t n = job.n, max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
-    for (int e = threadIdx.x; e < R * cols; e += blockDim.x) {
+    for (int e = threadIdx.x; e < kB; e += blockDim.x) {
         const int t = e / cols, c = e - t * cols;
         const int64_t key = lag_key((int64_t)t * kB + c0 + c, n, max_lag);
         if (key >= 0) best = better(best, Best{fabs(sm[e].x), key});
@@ -560,12 +578,20 @@ __global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__
     block_best(best, pv, pk, blockIdx.y);
 }
 
+// One warp per job: lanes stride over the candidates, then a shuffle
+// reduction (`better` is associative and commutative: the largest value,
+// ties to the smallest key, i.e. the CPU scan's first maximum).
 __global__ void pick_lag(const LagJob *__restrict__ jobs, int njobs, const double *pv, const int64_t *pk, int parts) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (j >= njobs) return;
     Best best{-INFINITY, INT64_MAX};
-    for (int p = 0; p < parts; ++p) best = better(best, Best{pv[(int64_t)j * parts + p], pk[(int64_t)j * parts + p]});
-    *jobs[j].lag_out = best.key == INT64_MAX ? 0 : best.key - (jobs[j].biggest - 1);
+    for (int p = lane; p < parts; p += 32)
+        best = better(best, Best{pv[(int64_t)j * parts + p], pk[(int64_t)j * parts + p]});
+    for (int off = 16; off > 0; off >>= 1) {
+        Best o{__shfl_down_sync(0xffffffffu, best.v, off), __shfl_down_sync(0xffffffffu, best.key, off)};
+        best = better(best, o);
+    }
+    if (lane == 0) *jobs[j].lag_out = best.key == INT64_MAX ? 0 : best.key - (jobs[j].biggest - 1);
 }
 
 }  // namespace
@@ -622,7 +648,7 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
             small_lag<true><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block, pv, pk);
         else
             small_lag<false><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block, pv, pk);
-        pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, 1);
+        pick_lag<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, pv, pk, 1);
         launch_counter() += 2;
         return;
     }
@@ -637,7 +663,7 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
     middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads, 2 * kPadB * sizeof(double2), s>>>(
         d_jobs, tst);
     inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);
-    pick_lag<<<(njobs + 127) / 128, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
+    pick_lag<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
     launch_counter() += 4;
 }
 

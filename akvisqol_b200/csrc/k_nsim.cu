@@ -166,6 +166,122 @@ __global__ void __launch_bounds__(kThreads) table_kernel(const TableTask *__rest
     t.out[off] = sum / (double)(nb * P);
 }
 
+// The fast forms' table with the patch width P known at compile time (30
+// in audio mode, 20 in speech mode) and W offsets per CTA. Same cells as
+// table_kernel<true, W> (the fast forms need not follow the CPU's operation
+// order), arranged for throughput:
+//
+// * the degraded plane's rows are streamed through shared memory, one band
+//   row at a time and double-buffered with asynchronous copies: row r needs
+//   the padded spectrogram's rows r-1, r, r+1 and the 3x3 mean, mean^2 and
+//   variance planes' row r over the CTA's columns [off0, off0 + W + P - 1);
+// * the 3x3 window of the ref x deg products uses per-column sums (the
+//   window is symmetric: corners, edges, centre), about 7 operations per
+//   cell at dependency depth ~4 instead of a 9-deep FMA chain;
+// * the cell's one quotient divides by a positive denominator with a
+//   reciprocal estimate refined by Newton-Raphson iterations (Markstein's
+//   refinement: r' = r + r(1 - d r), then q' = q + r'(n - d q)), which
+//   agrees with the IEEE quotient to about an ulp.
+__device__ inline double fast_quotient(double n, double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    r = __fma_rn(r, __fma_rn(-d, r, 1.0), r);
+    r = __fma_rn(r, __fma_rn(-d, r, 1.0), r);
+    const double q = n * r;
+    return __fma_rn(r, __fma_rn(-d, q, n), q);
+}
+
+__device__ inline double sim_cell_quick(double mr, double rms, double sr, double md, double dms, double sd,
+                                        double crd) {
+    const double mrd = mr * md;
+    const double srd = crd - mrd;
+    const double q = sr * sd;
+    const double sden = q < 0.0 ? kC3 : fabs(q) + kC3;
+    return fast_quotient(__fma_rn(2.0, mrd, kC1) * (srd + kC3), (rms + dms + kC1) * sden);
+}
+
+constexpr int kStageRows = 6;  // pad rows r-1, r, r+1; mu, dms, sds rows r
+
+__device__ inline void cp_async8(double *dst, const double *src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
+template <int P, int W>
+__global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restrict__ tasks, int nb) {
+    extern __shared__ __align__(16) double smf[];
+    constexpr int kSpan = W + P - 1;  // degraded columns a CTA reads
+    const TableTask t = tasks[blockIdx.x];
+    const int total = nb * P;
+    double *terms = smf;                   // 4 x nb x P
+    double *stage = smf + 4 * total;       // 2 buffers x kStageRows x kSpan
+    for (int e = threadIdx.x; e < 4 * total; e += W) terms[e] = t.ref_terms[e];
+    const int w = t.width;
+    auto fetch = [&](int r, int buf) {
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        double *dst = stage + buf * kStageRows * kSpan;
+        for (int e = threadIdx.x; e < kStageRows * kSpan; e += W) {
+            const int k = e / kSpan, col = t.off0 + (e - k * kSpan);
+            const int row = k == 0 ? rm : k == 2 ? rp : r;
+            const double *plane = k < 3 ? t.pad : k == 3 ? t.mu : k == 4 ? t.dms : t.sds;
+            const double *src = plane + (int64_t)row * w;
+            const bool in = col < w;
+            cp_async8(dst + e, in ? src + col : src, in ? 8 : 0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    fetch(0, 0);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    const double *rv = terms, *mr = terms + total, *rms = terms + 2 * total, *srs = terms + 3 * total;
+    const int64_t off = t.off0 + threadIdx.x;
+    double sum = 0.0;
+    for (int r = 0; r < nb; ++r) {
+        if (r + 1 < nb) fetch(r + 1, (r + 1) & 1);
+        const double *st = stage + (r & 1) * kStageRows * kSpan + threadIdx.x;
+        const double *pm = st, *p0 = st + kSpan, *pp = st + 2 * kSpan;
+        const double *mu = st + 3 * kSpan, *dm = st + 4 * kSpan, *sd = st + 5 * kSpan;
+        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
+        const double *qm = rv + rm * P, *q0 = rv + r * P, *qp = rv + rp * P;
+        // column sums of the ref x deg products: E = rows r-1 + r+1, M = row r
+        double Ec = qm[0] * pm[0] + qp[0] * pp[0], Mc = q0[0] * p0[0];
+        double Em = Ec, Mm = Mc;
+#pragma unroll
+        for (int c = 0; c < P; ++c) {
+            const int cp = c + 1 < P ? c + 1 : P - 1;
+            double Ep = Ec, Mp = Mc;
+            if (c + 1 < P) {
+                Ep = qm[cp] * pm[cp] + qp[cp] * pp[cp];
+                Mp = q0[cp] * p0[cp];
+            }
+            const double crd = __fma_rn(kW2, Mc, __fma_rn(kW1, (Mm + Mp) + Ec, kW0 * (Em + Ep)));
+            double md, dms, sds;
+            if (c == 0 || c == P - 1) {
+                const int cm = c == 0 ? 0 : c - 1;
+                const double d00 = pm[cm], d01 = pm[c], d02 = pm[cp];
+                const double d10 = p0[cm], d11 = p0[c], d12 = p0[cp];
+                const double d20 = pp[cm], d21 = pp[c], d22 = pp[cp];
+                md = taps9_fma(d00, d01, d02, d10, d11, d12, d20, d21, d22);
+                const double cdsq = taps9_fma(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12,
+                                              d20 * d20, d21 * d21, d22 * d22);
+                dms = md * md;
+                sds = signed_root(cdsq - dms);
+            } else {
+                md = mu[c];
+                dms = dm[c];
+                sds = sd[c];
+            }
+            const int ri = r * P + c;
+            sum += sim_cell_quick(mr[ri], rms[ri], srs[ri], md, dms, sds, crd);
+            Em = Ec, Mm = Mc;
+            Ec = Ep, Mc = Mp;
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+    }
+    if (off <= t.hi) t.out[off] = sum / (double)(nb * P);
+}
+
 // Per-band statistics of one patch pair, one thread per band row
 // (reference measurePatchSimilarity, src/nsim.zig:427-510). Cell values are
 // formed from the 3x3 neighbourhood on the fly and recomputed for the
@@ -271,11 +387,35 @@ void nsim_init_attributes() {
     cudaFuncSetAttribute(table_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(table_kernel<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(table_kernel<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_fast_kernel<30, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_fast_kernel<30, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_fast_kernel<20, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(table_fast_kernel<20, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s) {
     if (ntasks <= 0) return;
     const size_t smem = (size_t)4 * nb * P * sizeof(double);
+    if (fast && (P == 30 || P == 20) && (width == 128 || width == 256)) {
+        const size_t staged = smem + (size_t)2 * kStageRows * (width + P - 1) * sizeof(double);
+#define VQB_TABLE_FAST(PP, W) table_fast_kernel<PP, W><<<ntasks, W, staged, s>>>(d_tasks, nb);
+        if (P == 30) {
+            if (width == 256) {
+                VQB_TABLE_FAST(30, 256)
+            } else {
+                VQB_TABLE_FAST(30, 128)
+            }
+        } else {
+            if (width == 256) {
+                VQB_TABLE_FAST(20, 256)
+            } else {
+                VQB_TABLE_FAST(20, 128)
+            }
+        }
+#undef VQB_TABLE_FAST
+        launch_counter() += 1;
+        return;
+    }
 #define VQB_TABLE(W)                                                             \
     if (fast)                                                                    \
         table_kernel<true, W><<<ntasks, W, smem, s>>>(d_tasks, nb, P);           \

@@ -2,15 +2,17 @@
 // absolute -45 dB floor, a per-frame floor 45 dB under the frame's peak over
 // both spectrograms, then the joint minimum subtracted.
 //
-// One CTA per spectrogram pair. A thread owns whole frames (columns), so
-// the dB values and the per-frame floor need no exchange; max and min are
-// exact in any order, so the block reductions match the CPU's loops.
+// Two launches over all pairs: dB values and per-frame floors with one
+// warp per band and 32 frames per CTA (plus a partial joint minimum per
+// CTA), then the joint minimum subtracted. Max and min are exact in any
+// order, so the reductions match the CPU's loops bit for bit.
 //
 // log10 follows fdlibm's e_log10.c (Sun Microsystems), the formula the
 // CPU's glibc log10 evaluates: with x = 2^k * m, y = k (+1 below 1),
 // log10(x) = (y*log10_2lo + ivln10*log(m)) + y*log10_2hi, evaluated in that
 // order without FMA. The natural log is CUDA's; results agree with glibc
 // to the last bit except where the two natural logs differ by an ulp.
+#include <algorithm>
 #include <cfloat>
 
 #include "device.cuh"
@@ -61,54 +63,89 @@ __device__ inline double to_db(double v) {
 
 __device__ inline double dmax(double a, double b) { return fmax(a, b); }
 
-__global__ void __launch_bounds__(256) prep_kernel(const PrepJob *__restrict__ jobs, int nb) {
-    const PrepJob job = jobs[blockIdx.x];
+// Phase 1: one CTA per 32 frames of one spectrogram pair, one warp per
+// band with its lanes along frames (coalesced rows). Each value's dB, the
+// frame's floor (the maximum over both spectrograms' bands, a shared-memory
+// reduction) and the floored values are formed in registers and written
+// once; the CTA's minimum goes to part[job * nparts + blockIdx.x] (+inf
+// when the CTA holds no frame of this pair). Max and min are exact in any
+// order, so the results are the CPU loops' bit for bit.
+constexpr int kPrepCols = 32;
+
+__global__ void __launch_bounds__(1024) prep_db_kernel(const PrepJob *__restrict__ jobs, int nb,
+                                                       double *__restrict__ part, int nparts) {
+    __shared__ double colmax[32][kPrepCols + 1];
+    __shared__ double floor_db[kPrepCols];
+    __shared__ double wmin[32];
+    const PrepJob job = jobs[blockIdx.y];
+    const int b = threadIdx.x >> 5, j = threadIdx.x & 31;
+    const int c = blockIdx.x * kPrepCols + j;
     const int nfr = job.nfr, nfd = job.nfd;
     const int minf = nfr < nfd ? nfr : nfd;
-    const int maxf = nfr > nfd ? nfr : nfd;
-    double lo = INFINITY;
-    for (int c = threadIdx.x; c < maxf; c += blockDim.x) {
-        double col_max = -INFINITY;
-        for (int b = 0; b < nb; ++b) {
-            double r = 0, d = 0;
-            if (c < nfr) job.ref[(int64_t)b * nfr + c] = r = to_db(job.ref_in[(int64_t)b * nfr + c]);
-            if (c < nfd) job.deg[(int64_t)b * nfd + c] = d = to_db(job.deg_in[(int64_t)b * nfd + c]);
-            if (c < minf) {
-                const double m = dmax(r, d);
-                if (m > col_max) col_max = m;
-            }
-        }
-        if (c < minf) {
-            const double floor_db = col_max - kRelFloor;
-            for (int b = 0; b < nb; ++b) {
-                double &rv = job.ref[(int64_t)b * nfr + c];
-                if (rv < floor_db) rv = floor_db;
-                double &dv = job.deg[(int64_t)b * nfd + c];
-                if (dv < floor_db) dv = floor_db;
-            }
-        }
-        for (int b = 0; b < nb; ++b) {
-            if (c < nfr && job.ref[(int64_t)b * nfr + c] < lo) lo = job.ref[(int64_t)b * nfr + c];
-            if (c < nfd && job.deg[(int64_t)b * nfd + c] < lo) lo = job.deg[(int64_t)b * nfd + c];
-        }
+    double r = 0.0, d = 0.0;
+    if (c < nfr) r = to_db(job.ref_in[(int64_t)b * nfr + c]);
+    if (c < nfd) d = to_db(job.deg_in[(int64_t)b * nfd + c]);
+    colmax[b][j] = c < minf ? dmax(r, d) : -INFINITY;
+    __syncthreads();
+    if (b == 0) {
+        double m = -INFINITY;
+        for (int k = 0; k < nb; ++k)
+            if (colmax[k][j] > m) m = colmax[k][j];
+        floor_db[j] = m - kRelFloor;
     }
-    // Joint minimum (reference src/spectrogram.zig:56-66).
+    __syncthreads();
+    double lo = INFINITY;
+    if (c < minf) {
+        const double f = floor_db[j];
+        if (r < f) r = f;
+        if (d < f) d = f;
+    }
+    if (c < nfr) {
+        job.ref[(int64_t)b * nfr + c] = r;
+        if (r < lo) lo = r;
+    }
+    if (c < nfd) {
+        job.deg[(int64_t)b * nfd + c] = d;
+        if (d < lo) lo = d;
+    }
     for (int off = 16; off > 0; off >>= 1) {
         const double o = __shfl_down_sync(0xffffffffu, lo, off);
         if (o < lo) lo = o;
     }
-    __shared__ double wmin[8];
-    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = lo;
+    if (j == 0) wmin[b] = lo;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
-            if (wmin[w] < lo) lo = wmin[w];
-        wmin[0] = lo;
+        double m = INFINITY;
+        for (int k = 0; k < nb; ++k)
+            if (wmin[k] < m) m = wmin[k];
+        part[(int64_t)blockIdx.y * nparts + blockIdx.x] = m;
+    }
+}
+
+// Phase 2: the joint minimum (reference src/spectrogram.zig:56-66) from the
+// phase-1 parts, subtracted from every value of both spectrograms.
+__global__ void __launch_bounds__(256) prep_sub_kernel(const PrepJob *__restrict__ jobs, int nb,
+                                                       const double *__restrict__ part, int nparts) {
+    __shared__ double lo_s;
+    const PrepJob job = jobs[blockIdx.y];
+    if (threadIdx.x < 32) {
+        double lo = INFINITY;
+        for (int k = threadIdx.x; k < nparts; k += 32) {
+            const double v = part[(int64_t)blockIdx.y * nparts + k];
+            if (v < lo) lo = v;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, lo, off);
+            if (o < lo) lo = o;
+        }
+        if (threadIdx.x == 0) lo_s = lo;
     }
     __syncthreads();
-    lo = wmin[0];
-    for (int64_t e = threadIdx.x; e < (int64_t)nb * nfr; e += blockDim.x) job.ref[e] -= lo;
-    for (int64_t e = threadIdx.x; e < (int64_t)nb * nfd; e += blockDim.x) job.deg[e] -= lo;
+    const double lo = lo_s;
+    const int64_t nr = (int64_t)nb * job.nfr, nd = (int64_t)nb * job.nfd;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nr; e += stride) job.ref[e] -= lo;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nd; e += stride) job.deg[e] -= lo;
 }
 
 __global__ void log10_kernel(const double *x, int64_t n, double *out) {
@@ -118,10 +155,18 @@ __global__ void log10_kernel(const double *x, int64_t n, double *out) {
 
 }  // namespace
 
-void launch_prep(const PrepJob *d_jobs, int njobs, int nb, cudaStream_t s) {
-    if (njobs <= 0) return;
-    prep_kernel<<<njobs, 256, 0, s>>>(d_jobs, nb);
-    launch_counter() += 1;
+size_t prep_scratch_count(int njobs, int max_frames) {
+    return (size_t)njobs * (size_t)((max_frames + kPrepCols - 1) / kPrepCols);
+}
+
+void launch_prep(const PrepJob *d_jobs, int njobs, int nb, int max_frames, double *d_scratch, cudaStream_t s) {
+    if (njobs <= 0 || max_frames <= 0) return;
+    const int nparts = (max_frames + kPrepCols - 1) / kPrepCols;
+    prep_db_kernel<<<dim3((unsigned)nparts, (unsigned)njobs), 32 * nb, 0, s>>>(d_jobs, nb, d_scratch, nparts);
+    // about four values per thread of the larger spectrogram
+    const int sub_blocks = std::max(1, std::min(64, (nb * max_frames + 1023) / 1024));
+    prep_sub_kernel<<<dim3((unsigned)sub_blocks, (unsigned)njobs), 256, 0, s>>>(d_jobs, nb, d_scratch, nparts);
+    launch_counter() += 2;
 }
 
 void launch_log10(const double *x, int64_t n, double *out, cudaStream_t s) {

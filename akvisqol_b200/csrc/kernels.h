@@ -49,16 +49,15 @@ struct DpJob {
 };
 
 // Per-band coefficients of the fast gammatone forms (k_gammatone_fast.cu).
+// Every stage is a biquad with the band's pole pair and a numerator
+// normalised to 1 + beta z^-1; the numerator gains are one factor, post64.
 struct FastBandCoeffs {
-    // f32 form: stage 1 in f64, stages 2-4 in f32
-    double n0, n1, d1, d2;     // stage 1: gain-folded numerator and poles
-    double post;               // |a0^3|, the numerator gain of stages 2-4
-    float beta[3];             // stages 2-4 numerators 1 + beta z^-1
-    float p1h, p1l, p2h, p2l;  // poles d1, d2 as hi + lo f32 pairs
-    int32_t direct_i;          // 1: direct form I, 0: transposed direct form II
-    // f64 FMA form: all four stages direct form I with unit-leading numerators
-    double beta64[4];          // numerators 1 + beta64 z^-1
-    double post64;             // |a0^4 / gain|
+    double d1, d2;             // poles, all four stages
+    double beta64[4];          // f64 numerators of stages 1-4
+    double post64;             // |s1n0 a0^3|, applied to the RMS
+    float beta[2];             // f32 form: numerators of stages 3-4
+    float p1h, p1l, p2h, p2l;  // f32 form: poles d1, d2 as hi + lo f32 pairs
+    int32_t direct_i;          // f32 form: 1 direct form I, 0 transposed direct form II
 };
 
 // Arithmetic forms of the batch pipeline.
@@ -138,7 +137,10 @@ void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int nti
                              int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s);
 
 // k_spec.cu
-void launch_prep(const PrepJob *d_jobs, int njobs, int nb, cudaStream_t s);
+// Spectrogram preparation of njobs pairs (max_frames = the largest nfr or
+// nfd); d_scratch holds prep_scratch_count(njobs, max_frames) doubles.
+size_t prep_scratch_count(int njobs, int max_frames);
+void launch_prep(const PrepJob *d_jobs, int njobs, int nb, int max_frames, double *d_scratch, cudaStream_t s);
 void launch_log10(const double *x, int64_t n, double *out, cudaStream_t s);
 
 // k_nsim.cu

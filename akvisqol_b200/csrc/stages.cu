@@ -121,13 +121,16 @@ int visqol_b200_fft(double *buf, size_t n, int inverse) {
 }
 
 int visqol_b200_prepare_for_comparison(double *ref, double *deg, size_t nb, size_t nfr, size_t nfd) {
-    if ((!ref && nfr) || (!deg && nfd) || nb == 0) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    if ((!ref && nfr) || (!deg && nfd) || nb == 0 || nb > 32)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument (1 <= nb <= 32)");
     return guarded([&] {
         vqb::Engine &e = stage_engine();
         DBuf<double> ri(ref, nb * nfr), di(deg, nb * nfd), ro(nb * nfr), dout(nb * nfd);
         vqb::PrepJob pj{ri.p, di.p, ro.p, dout.p, (int32_t)nfr, (int32_t)nfd};
         DBuf<vqb::PrepJob> dj(&pj, 1);
-        vqb::launch_prep(dj.p, 1, (int)nb, e.stream());
+        const int max_frames = (int)std::max(nfr, nfd);
+        DBuf<double> scratch(std::max<size_t>(1, vqb::prep_scratch_count(1, max_frames)));
+        vqb::launch_prep(dj.p, 1, (int)nb, max_frames, scratch.p, e.stream());
         VQB_CUDA(cudaStreamSynchronize(e.stream()));
         ro.get(ref, nb * nfr);
         dout.get(deg, nb * nfd);

@@ -205,7 +205,7 @@ int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb,
 int visqol_b200_fft(double *buf, size_t n, int inverse);
 
 /* dB, per-frame floor, joint minimum in place (reference
- * src/spectrogram.zig:69-80). */
+ * src/spectrogram.zig:69-80); nb from 1 to 32 bands. */
 int visqol_b200_prepare_for_comparison(double *ref, double *deg, size_t nb,
                                        size_t nf_ref, size_t nf_deg);
 

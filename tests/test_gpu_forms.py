@@ -4,7 +4,7 @@
   statistics. It reorders rounding only, so MOS stays within 1e-10 and
   every discrete decision (lags, patch indices, DP offsets, realignment)
   matches.
-* fast: gammatone stages 2-4 in f32. MOS within 1e-6 on the 10 s 48 kHz
+* fast: gammatone stages 3-4 in f32. MOS within 1e-6 on the 10 s 48 kHz
   audio workload; on low-SNR pairs whose upper bands hold flat white noise
   NSIM's structure term amplifies f32 rounding, and the stated bound there is
   1e-5. Lags, patch indices (VAD in speech mode) and matched offsets must
