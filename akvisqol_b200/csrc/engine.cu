@@ -291,7 +291,20 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
                 const size_t parts = fused_lag_parts(n);
                 double *pv = arena_.alloc_n<double>(parts * cnt);
                 int64_t *pk = arena_.alloc_n<int64_t>(parts * cnt);
-                launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, tw.stages, pv, pk, stream_);
+                auto launch = [&](int columns) {
+                    launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, tw.stages, pv, pk, columns, stream_);
+                };
+                // column passes: shared-memory tiles or registers, measured per
+                // transform size (VISQOL_LAG_COLUMNS=0/1 fixes the choice)
+                int columns = 0;
+                if (fused_lag_register_columns(n)) {
+                    const char *env = std::getenv("VISQOL_LAG_COLUMNS");
+                    columns = env && (env[0] == '0' || env[0] == '1')
+                                  ? env[0] - '0'
+                                  : tuned(kTuneLagColumns, (int)std::log2((double)n), raw ? 1 : 0, {1, 0}, launch,
+                                          stream_);
+                }
+                launch(columns);
                 continue;
             }
             const int parts = argmax_parts(n);

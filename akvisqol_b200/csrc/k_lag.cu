@@ -539,6 +539,152 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
     block_best(best, pv, pk, (int64_t)blockIdx.y * parts + blockIdx.x);
 }
 
+// Register forms of passes 1 and 3 for R = 2^G rows with 4 <= G <= 8 (the
+// global lag search of signals up to 2^19 samples, the 48 kHz realignment
+// slices, speech). Thread (c, j) of a CTA (c fastest: coalesced rows) keeps
+// 16 points of column c in registers: rows j + S m (S = R / 16) for the
+// spans R/2 .. R/16, then, after one shared-memory exchange, rows 16 j + m
+// for the spans 8 .. 1. Each stage's butterflies are the radix-2 ones of the
+// shared-memory passes, with the same twiddles, so the results are the same
+// bits; a pass costs one barrier instead of one per stage pair.
+template <int G>
+__device__ inline void dif_span_group_a(double2 (&x)[16], int j, const double2 *__restrict__ tcol, int64_t col) {
+    constexpr int R = 1 << G, S = R / 16;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const int half = 8 >> l;
+        const double2 *tw = tcol + tcol_off(G, l) + col;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & half) continue;
+            const double2 w = __ldg(tw + (int64_t)(j + S * (m & (half - 1))) * kB);
+            const double2 a = x[m], b = x[m + half];
+            x[m] = cadd(a, b);
+            x[m + half] = cmul(csub(a, b), w);
+        }
+    }
+}
+
+template <int G>
+__device__ inline void dif_span_group_b(double2 (&x)[16], const double2 *__restrict__ tcol, int64_t col) {
+    constexpr int R = 1 << G;
+#pragma unroll
+    for (int l = 4; l < G; ++l) {
+        const int h = R >> (l + 1);
+        const double2 *tw = tcol + tcol_off(G, l) + col;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & h) continue;
+            const double2 w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
+            const double2 a = x[m], b = x[m + h];
+            x[m] = cadd(a, b);
+            x[m + h] = cmul(csub(a, b), w);
+        }
+    }
+}
+
+template <int G>
+__device__ inline void dit_span_group_b(double2 (&x)[16], const double2 *__restrict__ tcol, int64_t col) {
+    constexpr int R = 1 << G;
+#pragma unroll
+    for (int l = G - 1; l >= 4; --l) {
+        const int h = R >> (l + 1);
+        const double2 *tw = tcol + tcol_off(G, l) + col;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & h) continue;
+            const double2 w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
+            const double2 a = x[m], b = cmul_conj(x[m + h], w);
+            x[m] = cadd(a, b);
+            x[m + h] = csub(a, b);
+        }
+    }
+}
+
+template <int G>
+__device__ inline void dit_span_group_a(double2 (&x)[16], int j, const double2 *__restrict__ tcol, int64_t col) {
+    constexpr int R = 1 << G, S = R / 16;
+#pragma unroll
+    for (int l = 3; l >= 0; --l) {
+        const int half = 8 >> l;
+        const double2 *tw = tcol + tcol_off(G, l) + col;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            if (m & half) continue;
+            const double2 w = __ldg(tw + (int64_t)(j + S * (m & (half - 1))) * kB);
+            const double2 a = x[m], b = cmul_conj(x[m + half], w);
+            x[m] = cadd(a, b);
+            x[m + half] = csub(a, b);
+        }
+    }
+}
+
+template <int G, bool RAW>
+__global__ void __launch_bounds__(kThreads) fwd_columns_reg(const LagJob *__restrict__ jobs,
+                                                            const double2 *__restrict__ tcol) {
+    extern __shared__ double2 sm[];
+    constexpr int R = 1 << G, cols = kB >> G, S = R / 16;
+    const LagJob job = jobs[blockIdx.y];
+    const int c = threadIdx.x % cols, j = threadIdx.x / cols;
+    const int64_t col = (int64_t)blockIdx.x * cols + c;
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    double2 x[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) x[m] = packed<RAW>(job, pa, pb, (int64_t)(j + S * m) * kB + col);
+    dif_span_group_a<G>(x, j, tcol, col);
+    if (G > 4) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) sm[(j + S * m) * cols + c] = x[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[(16 * j + m) * cols + c];
+        dif_span_group_b<G>(x, tcol, col);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) job.z[(int64_t)(16 * j + m) * kB + col] = x[m];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) job.z[(int64_t)(j + S * m) * kB + col] = x[m];
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kThreads) inv_columns_reg(const LagJob *__restrict__ jobs,
+                                                            const double2 *__restrict__ tcol, double *pv,
+                                                            int64_t *pk, int parts) {
+    extern __shared__ double2 sm[];
+    constexpr int R = 1 << G, cols = kB >> G, S = R / 16;
+    const LagJob job = jobs[blockIdx.y];
+    const int c = threadIdx.x % cols, j = threadIdx.x / cols;
+    const int64_t col = (int64_t)blockIdx.x * cols + c;
+    double2 x[16];
+    if (G > 4) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)(16 * j + m) * kB + col];
+        dit_span_group_b<G>(x, tcol, col);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) sm[(16 * j + m) * cols + c] = x[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[(j + S * m) * cols + c];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)(j + S * m) * kB + col];
+    }
+    dit_span_group_a<G>(x, j, tcol, col);
+    const int64_t n = job.n, max_lag = job.biggest - 1;
+    Best best{-INFINITY, INT64_MAX};
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int64_t key = lag_key((int64_t)(j + S * m) * kB + col, n, max_lag);
+        if (key >= 0) best = better(best, Best{fabs(x[m].x), key});
+    }
+    block_best(best, pv, pk, (int64_t)blockIdx.y * parts + blockIdx.x);
+}
+
 // Single-block transforms (n <= 4096): pack, DIF, cross, DIT, argmax in one CTA.
 template <bool RAW>
 __global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__ jobs, const double2 *__restrict__ tw,
@@ -601,6 +747,15 @@ void lag_init_attributes() {
     cudaFuncSetAttribute(fwd_columns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(fwd_columns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(inv_columns_argmax, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+#define VQB_COLS_ATTR(GG)                                                                        \
+    cudaFuncSetAttribute(fwd_columns_reg<GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);  \
+    cudaFuncSetAttribute(fwd_columns_reg<GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+    cudaFuncSetAttribute(inv_columns_reg<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    VQB_COLS_ATTR(5)
+    VQB_COLS_ATTR(6)
+    VQB_COLS_ATTR(7)
+    VQB_COLS_ATTR(8)
+#undef VQB_COLS_ATTR
     cudaFuncSetAttribute(small_lag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(small_lag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(middle_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -638,8 +793,11 @@ void fill_column_twiddles(const double2 *top, int64_t n, double2 *out) {
             for (int64_t col = 0; col < kB; ++col) out[k++] = top[(m * kB + col) << l];
 }
 
+bool fused_lag_register_columns(int64_t n) { return n >= ((int64_t)kB << 4) && n <= ((int64_t)kB << 8); }
+
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
-                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, cudaStream_t s) {
+                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
+                      cudaStream_t s) {
     if (njobs <= 0) return;
     const size_t one = (size_t)kB * sizeof(double2);
     if (n <= kB) {
@@ -656,13 +814,45 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
     for (int64_t r = n / kB; r > 1; r >>= 1) ++G;
     const int parts = (int)fused_lag_parts(n);
     const int64_t nblk = n / kB;
-    if (raw)
-        fwd_columns<true><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
-    else
-        fwd_columns<false><<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol);
+    const dim3 grid((unsigned)parts, (unsigned)njobs);
+    const size_t reg_smem = G > 4 ? one : 0;
+    const int Gr = columns == 1 ? G : 0;  // 0: no register pass, the shared-memory one
+    switch (Gr) {
+#define VQB_COLS(GG)                                                                                       \
+    case GG:                                                                                               \
+        if (raw)                                                                                           \
+            fwd_columns_reg<GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);                      \
+        else                                                                                               \
+            fwd_columns_reg<GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);                     \
+        break;
+        VQB_COLS(4)
+        VQB_COLS(5)
+        VQB_COLS(6)
+        VQB_COLS(7)
+        VQB_COLS(8)
+#undef VQB_COLS
+    default:
+        if (raw)
+            fwd_columns<true><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+        else
+            fwd_columns<false><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+    }
     middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads, 2 * kPadB * sizeof(double2), s>>>(
         d_jobs, tst);
-    inv_columns_argmax<<<dim3((unsigned)parts, (unsigned)njobs), kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);
+    switch (Gr) {
+#define VQB_COLS(GG)                                                                                       \
+    case GG:                                                                                               \
+        inv_columns_reg<GG><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol, pv, pk, parts);                \
+        break;
+        VQB_COLS(4)
+        VQB_COLS(5)
+        VQB_COLS(6)
+        VQB_COLS(7)
+        VQB_COLS(8)
+#undef VQB_COLS
+    default:
+        inv_columns_argmax<<<grid, kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);
+    }
     pick_lag<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
     launch_counter() += 4;
 }

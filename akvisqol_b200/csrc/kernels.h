@@ -111,8 +111,12 @@ void fill_column_twiddles(const double2 *top, int64_t n, double2 *out);
 // (block[k] = W_4096^k): block_stage_twiddle_count() entries.
 size_t block_stage_twiddle_count();
 void fill_block_stage_twiddles(const double2 *block, double2 *out);
+// columns: 0 = the shared-memory column passes (any n), 1 = the register
+// ones (only where fused_lag_register_columns(n); else as 0). Same results.
+bool fused_lag_register_columns(int64_t n);
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
-                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, cudaStream_t s);
+                      const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
+                      cudaStream_t s);
 
 // k_gammatone.cu
 int gammatone_frames_per_cta(int nb);

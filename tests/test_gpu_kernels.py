@@ -63,6 +63,23 @@ def test_lags_random(native, oracle):
         assert native.envelope_lag(a, b) == oracle.envelope_lag(a, b)
 
 
+@pytest.mark.parametrize("columns", ["0", "1"])
+@pytest.mark.parametrize("rows_log2", [3, 4, 5, 6, 7, 8, 9])
+def test_lags_column_pass_sizes(native, oracle, rows_log2, columns, monkeypatch):
+    """Signal lengths whose transforms have 2^rows_log2 rows of 4096 points,
+    with each column-pass implementation: shared-memory tiles (0) and, for
+    4..8 rows_log2, registers (1)."""
+    monkeypatch.setenv("VISQOL_LAG_COLUMNS", columns)
+    n = 4096 << rows_log2
+    rng = np.random.default_rng(100 + rows_log2)
+    la = int(0.4 * n)
+    a = rng.uniform(-1, 1, la)
+    shift = int(rng.integers(1, 400))
+    b = np.concatenate([np.zeros(shift), a])[:la + 57] + 0.05 * rng.standard_normal(la + 57)
+    assert native.best_lag(a, b) == oracle.best_lag(a, b)
+    assert native.envelope_lag(a, b) == oracle.envelope_lag(a, b)
+
+
 def test_envelope_lag_full_pair(native, oracle, audio0):
     ref, deg = audio0
     assert native.envelope_lag(ref, deg) == oracle.envelope_lag(ref, deg)
