@@ -539,93 +539,92 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
     block_best(best, pv, pk, (int64_t)blockIdx.y * parts + blockIdx.x);
 }
 
-// Register forms of passes 1 and 3 for R = 2^G rows with 4 <= G <= 8 (the
-// global lag search of signals up to 2^19 samples, the 48 kHz realignment
-// slices, speech). Thread (c, j) of a CTA (c fastest: coalesced rows) keeps
-// 16 points of column c in registers: rows j + S m (S = R / 16) for the
-// spans R/2 .. R/16, then, after one shared-memory exchange, rows 16 j + m
-// for the spans 8 .. 1. Each stage's butterflies are the radix-2 ones of the
-// shared-memory passes, with the same twiddles, so the results are the same
-// bits; a pass costs one barrier instead of one per stage pair.
-template <int G>
-__device__ inline void dif_span_group_a(double2 (&x)[16], int j, const double2 *__restrict__ tcol, int64_t col) {
-    constexpr int R = 1 << G, S = R / 16;
+// Register forms of passes 1 and 3 for R = 2^G rows, 4 <= G <= 11 (signals up to 2^22 samples). Thread
+// q of a column (c, q: c fastest, so rows are coalesced) keeps 16 points of
+// column c in registers, and the G column stages run in groups of four:
+//
+//   group A (spans R/2 .. R/16):    rows q + (R/16) m
+//   group B (spans R/32 .. R/256):  rows b (R/16) + q' + (R/256) m, with
+//                                   q = b (R/256) + q'   (only if G > 8)
+//   tail (spans <= 8):              rows 16 q + m
+//
+// with one shared-memory exchange between groups. Each stage's butterflies
+// are the radix-2 ones of the shared-memory passes, with the same twiddles
+// (stage l, lower row t: tcol[off(l) + (t mod 2h) 4096 + col]), so the
+// results are the same bits; a group costs one barrier instead of one per
+// stage pair.
+template <int G, bool DIT>
+__device__ inline void column_group4(double2 (&x)[16], int l0, int stride, int base_mod,
+                                     const double2 *__restrict__ tcol, int64_t col) {
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-        const int half = 8 >> l;
+    for (int kk = 0; kk < 4; ++kk) {
+        const int k = DIT ? 3 - kk : kk;
+        const int l = l0 + k, half = 8 >> k;
         const double2 *tw = tcol + tcol_off(G, l) + col;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const double2 w = __ldg(tw + (int64_t)(j + S * (m & (half - 1))) * kB);
-            const double2 a = x[m], b = x[m + half];
-            x[m] = cadd(a, b);
-            x[m + half] = cmul(csub(a, b), w);
+            const double2 w = __ldg(tw + (int64_t)(base_mod + stride * (m & (half - 1))) * kB);
+            const double2 a = x[m];
+            if (!DIT) {
+                const double2 b = x[m + half];
+                x[m] = cadd(a, b);
+                x[m + half] = cmul(csub(a, b), w);
+            } else {
+                const double2 b = cmul_conj(x[m + half], w);
+                x[m] = cadd(a, b);
+                x[m + half] = csub(a, b);
+            }
         }
     }
 }
 
-template <int G>
-__device__ inline void dif_span_group_b(double2 (&x)[16], const double2 *__restrict__ tcol, int64_t col) {
+// Stages l0 .. G-1, whose spans h = R >> (l+1) are at most 8, on rows
+// 16 q + m (t mod 2h = m mod 2h).
+template <int G, bool DIT>
+__device__ inline void column_tail(double2 (&x)[16], int l0, const double2 *__restrict__ tcol, int64_t col) {
     constexpr int R = 1 << G;
 #pragma unroll
-    for (int l = 4; l < G; ++l) {
+    for (int kk = 0; kk < 4; ++kk) {
+        const int l = DIT ? G - 1 - kk : l0 + kk;
+        if (l < l0 || l >= G) continue;
         const int h = R >> (l + 1);
         const double2 *tw = tcol + tcol_off(G, l) + col;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & h) continue;
             const double2 w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
-            const double2 a = x[m], b = x[m + h];
-            x[m] = cadd(a, b);
-            x[m + h] = cmul(csub(a, b), w);
+            const double2 a = x[m];
+            if (!DIT) {
+                const double2 b = x[m + h];
+                x[m] = cadd(a, b);
+                x[m + h] = cmul(csub(a, b), w);
+            } else {
+                const double2 b = cmul_conj(x[m + h], w);
+                x[m] = cadd(a, b);
+                x[m + h] = csub(a, b);
+            }
         }
     }
 }
 
+// Row of register m in group A, group B and the tail, for thread q.
 template <int G>
-__device__ inline void dit_span_group_b(double2 (&x)[16], const double2 *__restrict__ tcol, int64_t col) {
-    constexpr int R = 1 << G;
-#pragma unroll
-    for (int l = G - 1; l >= 4; --l) {
-        const int h = R >> (l + 1);
-        const double2 *tw = tcol + tcol_off(G, l) + col;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            if (m & h) continue;
-            const double2 w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
-            const double2 a = x[m], b = cmul_conj(x[m + h], w);
-            x[m] = cadd(a, b);
-            x[m + h] = csub(a, b);
-        }
-    }
-}
-
+__device__ inline int row_a(int q, int m) { return q + ((1 << G) / 16) * m; }
 template <int G>
-__device__ inline void dit_span_group_a(double2 (&x)[16], int j, const double2 *__restrict__ tcol, int64_t col) {
-    constexpr int R = 1 << G, S = R / 16;
-#pragma unroll
-    for (int l = 3; l >= 0; --l) {
-        const int half = 8 >> l;
-        const double2 *tw = tcol + tcol_off(G, l) + col;
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            if (m & half) continue;
-            const double2 w = __ldg(tw + (int64_t)(j + S * (m & (half - 1))) * kB);
-            const double2 a = x[m], b = cmul_conj(x[m + half], w);
-            x[m] = cadd(a, b);
-            x[m + half] = csub(a, b);
-        }
-    }
+__device__ inline int row_b(int q, int m) {
+    constexpr int R = 1 << G, s = R / 256 > 0 ? R / 256 : 1;
+    return (q / s) * (R / 16) + (q % s) + s * m;
 }
+__device__ inline int row_t(int q, int m) { return 16 * q + m; }
 
 template <int G, bool RAW>
-__global__ void __launch_bounds__(kThreads) fwd_columns_reg(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, 2) fwd_columns_reg(const LagJob *__restrict__ jobs,
                                                             const double2 *__restrict__ tcol) {
     extern __shared__ double2 sm[];
-    constexpr int R = 1 << G, cols = kB >> G, S = R / 16;
+    constexpr int R = 1 << G, cols = kB >> G;
     const LagJob job = jobs[blockIdx.y];
-    const int c = threadIdx.x % cols, j = threadIdx.x / cols;
+    const int c = threadIdx.x % cols, q = threadIdx.x / cols;
     const int64_t col = (int64_t)blockIdx.x * cols + c;
     EnvParams pa{}, pb{};
     if (!RAW) {
@@ -634,52 +633,70 @@ __global__ void __launch_bounds__(kThreads) fwd_columns_reg(const LagJob *__rest
     }
     double2 x[16];
 #pragma unroll
-    for (int m = 0; m < 16; ++m) x[m] = packed<RAW>(job, pa, pb, (int64_t)(j + S * m) * kB + col);
-    dif_span_group_a<G>(x, j, tcol, col);
+    for (int m = 0; m < 16; ++m) x[m] = packed<RAW>(job, pa, pb, (int64_t)row_a<G>(q, m) * kB + col);
+    column_group4<G, false>(x, 0, R / 16, q, tcol, col);
     if (G > 4) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) sm[(j + S * m) * cols + c] = x[m];
+        for (int m = 0; m < 16; ++m) sm[row_a<G>(q, m) * cols + c] = x[m];
         __syncthreads();
+        if (G > 8) {
+            constexpr int s = R / 256 > 0 ? R / 256 : 1;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = sm[(16 * j + m) * cols + c];
-        dif_span_group_b<G>(x, tcol, col);
+            for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
+            column_group4<G, false>(x, 4, s, q % s, tcol, col);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) job.z[(int64_t)(16 * j + m) * kB + col] = x[m];
+            for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[row_t(q, m) * cols + c];
+        column_tail<G, false>(x, G > 8 ? 8 : 4, tcol, col);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) job.z[(int64_t)row_t(q, m) * kB + col] = x[m];
     } else {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) job.z[(int64_t)(j + S * m) * kB + col] = x[m];
+        for (int m = 0; m < 16; ++m) job.z[(int64_t)row_a<G>(q, m) * kB + col] = x[m];
     }
 }
 
 template <int G>
-__global__ void __launch_bounds__(kThreads) inv_columns_reg(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__restrict__ jobs,
                                                             const double2 *__restrict__ tcol, double *pv,
                                                             int64_t *pk, int parts) {
     extern __shared__ double2 sm[];
-    constexpr int R = 1 << G, cols = kB >> G, S = R / 16;
+    constexpr int R = 1 << G, cols = kB >> G;
     const LagJob job = jobs[blockIdx.y];
-    const int c = threadIdx.x % cols, j = threadIdx.x / cols;
+    const int c = threadIdx.x % cols, q = threadIdx.x / cols;
     const int64_t col = (int64_t)blockIdx.x * cols + c;
     double2 x[16];
     if (G > 4) {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)(16 * j + m) * kB + col];
-        dit_span_group_b<G>(x, tcol, col);
+        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)row_t(q, m) * kB + col];
+        column_tail<G, true>(x, G > 8 ? 8 : 4, tcol, col);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) sm[(16 * j + m) * cols + c] = x[m];
+        for (int m = 0; m < 16; ++m) sm[row_t(q, m) * cols + c] = x[m];
         __syncthreads();
+        if (G > 8) {
+            constexpr int s = R / 256 > 0 ? R / 256 : 1;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = sm[(j + S * m) * cols + c];
+            for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
+            column_group4<G, true>(x, 4, s, q % s, tcol, col);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[row_a<G>(q, m) * cols + c];
     } else {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)(j + S * m) * kB + col];
+        for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)row_a<G>(q, m) * kB + col];
     }
-    dit_span_group_a<G>(x, j, tcol, col);
+    column_group4<G, true>(x, 0, R / 16, q, tcol, col);
     const int64_t n = job.n, max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
-        const int64_t key = lag_key((int64_t)(j + S * m) * kB + col, n, max_lag);
+        const int64_t key = lag_key((int64_t)row_a<G>(q, m) * kB + col, n, max_lag);
         if (key >= 0) best = better(best, Best{fabs(x[m].x), key});
     }
     block_best(best, pv, pk, (int64_t)blockIdx.y * parts + blockIdx.x);
@@ -755,6 +772,9 @@ void lag_init_attributes() {
     VQB_COLS_ATTR(6)
     VQB_COLS_ATTR(7)
     VQB_COLS_ATTR(8)
+    VQB_COLS_ATTR(9)
+    VQB_COLS_ATTR(10)
+    VQB_COLS_ATTR(11)
 #undef VQB_COLS_ATTR
     cudaFuncSetAttribute(small_lag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(small_lag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
@@ -793,7 +813,7 @@ void fill_column_twiddles(const double2 *top, int64_t n, double2 *out) {
             for (int64_t col = 0; col < kB; ++col) out[k++] = top[(m * kB + col) << l];
 }
 
-bool fused_lag_register_columns(int64_t n) { return n >= ((int64_t)kB << 4) && n <= ((int64_t)kB << 8); }
+bool fused_lag_register_columns(int64_t n) { return n >= ((int64_t)kB << 4) && n <= ((int64_t)kB << 11); }
 
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
                       const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
@@ -830,6 +850,9 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
         VQB_COLS(6)
         VQB_COLS(7)
         VQB_COLS(8)
+        VQB_COLS(9)
+        VQB_COLS(10)
+        VQB_COLS(11)
 #undef VQB_COLS
     default:
         if (raw)
@@ -849,6 +872,9 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
         VQB_COLS(6)
         VQB_COLS(7)
         VQB_COLS(8)
+        VQB_COLS(9)
+        VQB_COLS(10)
+        VQB_COLS(11)
 #undef VQB_COLS
     default:
         inv_columns_argmax<<<grid, kThreads, one, s>>>(d_jobs, G, tcol, pv, pk, parts);

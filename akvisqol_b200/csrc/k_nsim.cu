@@ -171,10 +171,13 @@ __global__ void __launch_bounds__(kThreads) table_kernel(const TableTask *__rest
 // table_kernel<true, W> (the fast forms need not follow the CPU's operation
 // order), arranged for throughput:
 //
-// * the degraded plane's rows are streamed through shared memory, one band
-//   row at a time and double-buffered with asynchronous copies: row r needs
-//   the padded spectrogram's rows r-1, r, r+1 and the 3x3 mean, mean^2 and
-//   variance planes' row r over the CTA's columns [off0, off0 + W + P - 1);
+// * the degraded plane's rows and the reference terms' rows are streamed
+//   through shared memory, one band row at a time and double-buffered with
+//   asynchronous copies: row r needs the padded spectrogram's rows r-1, r,
+//   r+1 and the 3x3 mean, mean^2 and variance planes' row r over the CTA's
+//   columns [off0, off0 + W + P - 1), and the same rows of the reference
+//   patch's terms (about 18 KB of shared memory per CTA at W = 128, so
+//   that register use, not shared memory, bounds the CTAs per SM);
 // * the 3x3 window of the ref x deg products uses per-column sums (the
 //   window is symmetric: corners, edges, centre), about 7 operations per
 //   cell at dependency depth ~4 instead of a 9-deep FMA chain;
@@ -210,16 +213,17 @@ __device__ inline void cp_async8(double *dst, const double *src, int bytes) {
 template <int P, int W>
 __global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restrict__ tasks, int nb) {
     extern __shared__ __align__(16) double smf[];
-    constexpr int kSpan = W + P - 1;  // degraded columns a CTA reads
+    constexpr int kSpan = W + P - 1;                        // degraded columns a CTA reads
+    constexpr int kStage = kStageRows * kSpan + kStageRows * P;  // one band row's stage
     const TableTask t = tasks[blockIdx.x];
     const int total = nb * P;
-    double *terms = smf;                   // 4 x nb x P
-    double *stage = smf + 4 * total;       // 2 buffers x kStageRows x kSpan
-    for (int e = threadIdx.x; e < 4 * total; e += W) terms[e] = t.ref_terms[e];
     const int w = t.width;
+    // Row r's stage: the degraded plane's rows (pad r-1, r, r+1; mu, dms, sds
+    // r) over the CTA's columns, then the reference terms' rows (values r-1,
+    // r, r+1; mean, mean^2, variance r) over the patch's P columns.
     auto fetch = [&](int r, int buf) {
         const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
-        double *dst = stage + buf * kStageRows * kSpan;
+        double *dst = smf + buf * kStage;
         for (int e = threadIdx.x; e < kStageRows * kSpan; e += W) {
             const int k = e / kSpan, col = t.off0 + (e - k * kSpan);
             const int row = k == 0 ? rm : k == 2 ? rp : r;
@@ -228,21 +232,28 @@ __global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restri
             const bool in = col < w;
             cp_async8(dst + e, in ? src + col : src, in ? 8 : 0);
         }
+        double *tdst = dst + kStageRows * kSpan;
+        for (int e = threadIdx.x; e < kStageRows * P; e += W) {
+            const int k = e / P, c = e - k * P;
+            const int row = k == 0 ? rm : k == 2 ? rp : r;
+            const int term = k < 3 ? 0 : k - 2;  // values, mean, mean^2, variance
+            cp_async8(tdst + e, t.ref_terms + term * total + row * P + c, 8);
+        }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     fetch(0, 0);
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    const double *rv = terms, *mr = terms + total, *rms = terms + 2 * total, *srs = terms + 3 * total;
     const int64_t off = t.off0 + threadIdx.x;
     double sum = 0.0;
     for (int r = 0; r < nb; ++r) {
         if (r + 1 < nb) fetch(r + 1, (r + 1) & 1);
-        const double *st = stage + (r & 1) * kStageRows * kSpan + threadIdx.x;
+        const double *stg = smf + (r & 1) * kStage;
+        const double *st = stg + threadIdx.x;
         const double *pm = st, *p0 = st + kSpan, *pp = st + 2 * kSpan;
         const double *mu = st + 3 * kSpan, *dm = st + 4 * kSpan, *sd = st + 5 * kSpan;
-        const int rm = r == 0 ? 0 : r - 1, rp = r + 1 >= nb ? nb - 1 : r + 1;
-        const double *qm = rv + rm * P, *q0 = rv + r * P, *qp = rv + rp * P;
+        const double *tr = stg + kStageRows * kSpan;
+        const double *qm = tr, *q0 = tr + P, *qp = tr + 2 * P, *mr = tr + 3 * P, *rms = tr + 4 * P, *srs = tr + 5 * P;
         // column sums of the ref x deg products: E = rows r-1 + r+1, M = row r
         double Ec = qm[0] * pm[0] + qp[0] * pp[0], Mc = q0[0] * p0[0];
         double Em = Ec, Mm = Mc;
@@ -271,8 +282,7 @@ __global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restri
                 dms = dm[c];
                 sds = sd[c];
             }
-            const int ri = r * P + c;
-            sum += sim_cell_quick(mr[ri], rms[ri], srs[ri], md, dms, sds, crd);
+            sum += sim_cell_quick(mr[c], rms[c], srs[c], md, dms, sds, crd);
             Em = Ec, Mm = Mc;
             Ec = Ep, Mc = Mp;
         }
@@ -397,7 +407,7 @@ void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast
     if (ntasks <= 0) return;
     const size_t smem = (size_t)4 * nb * P * sizeof(double);
     if (fast && (P == 30 || P == 20) && (width == 128 || width == 256)) {
-        const size_t staged = smem + (size_t)2 * kStageRows * (width + P - 1) * sizeof(double);
+        const size_t staged = (size_t)2 * kStageRows * ((width + P - 1) + P) * sizeof(double);
 #define VQB_TABLE_FAST(PP, W) table_fast_kernel<PP, W><<<ntasks, W, staged, s>>>(d_tasks, nb);
         if (P == 30) {
             if (width == 256) {
