@@ -166,10 +166,12 @@ __global__ void __launch_bounds__(kThreads) table_kernel(const TableTask *__rest
     t.out[off] = sum / (double)(nb * P);
 }
 
-// The fast forms' table with the patch width P known at compile time (30
-// in audio mode, 20 in speech mode) and W offsets per CTA. Same cells as
-// table_kernel<true, W> (the fast forms need not follow the CPU's operation
-// order), arranged for throughput:
+// The table with the patch width P known at compile time (30 in audio
+// mode, 20 in speech mode) and W offsets per CTA. The exact form (kFast
+// false) computes the cells of table_kernel<false, W> with the same
+// operations in the same order; the fast forms (kFast true) compute
+// table_kernel<true, W>'s cells, which need not follow the CPU's order,
+// arranged for throughput:
 //
 // * the degraded plane's rows and the reference terms' rows are streamed
 //   through shared memory, one band row at a time and double-buffered with
@@ -210,8 +212,8 @@ __device__ inline void cp_async8(double *dst, const double *src, int bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 
-template <int P, int W>
-__global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restrict__ tasks, int nb) {
+template <bool kFast, int P, int W>
+__global__ void __launch_bounds__(W) table_staged_kernel(const TableTask *__restrict__ tasks, int nb) {
     extern __shared__ __align__(16) double smf[];
     constexpr int kSpan = W + P - 1;                        // degraded columns a CTA reads
     constexpr int kStage = kStageRows * kSpan + kStageRows * P;  // one band row's stage
@@ -254,37 +256,70 @@ __global__ void __launch_bounds__(W) table_fast_kernel(const TableTask *__restri
         const double *mu = st + 3 * kSpan, *dm = st + 4 * kSpan, *sd = st + 5 * kSpan;
         const double *tr = stg + kStageRows * kSpan;
         const double *qm = tr, *q0 = tr + P, *qp = tr + 2 * P, *mr = tr + 3 * P, *rms = tr + 4 * P, *srs = tr + 5 * P;
-        // column sums of the ref x deg products: E = rows r-1 + r+1, M = row r
-        double Ec = qm[0] * pm[0] + qp[0] * pp[0], Mc = q0[0] * p0[0];
-        double Em = Ec, Mm = Mc;
+        if (kFast) {
+            // column sums of the ref x deg products: E = rows r-1 + r+1, M = row r
+            double Ec = qm[0] * pm[0] + qp[0] * pp[0], Mc = q0[0] * p0[0];
+            double Em = Ec, Mm = Mc;
 #pragma unroll
-        for (int c = 0; c < P; ++c) {
-            const int cp = c + 1 < P ? c + 1 : P - 1;
-            double Ep = Ec, Mp = Mc;
-            if (c + 1 < P) {
-                Ep = qm[cp] * pm[cp] + qp[cp] * pp[cp];
-                Mp = q0[cp] * p0[cp];
+            for (int c = 0; c < P; ++c) {
+                const int cp = c + 1 < P ? c + 1 : P - 1;
+                double Ep = Ec, Mp = Mc;
+                if (c + 1 < P) {
+                    Ep = qm[cp] * pm[cp] + qp[cp] * pp[cp];
+                    Mp = q0[cp] * p0[cp];
+                }
+                const double crd = __fma_rn(kW2, Mc, __fma_rn(kW1, (Mm + Mp) + Ec, kW0 * (Em + Ep)));
+                double md, dms, sds;
+                if (c == 0 || c == P - 1) {
+                    const int cm = c == 0 ? 0 : c - 1;
+                    const double d00 = pm[cm], d01 = pm[c], d02 = pm[cp];
+                    const double d10 = p0[cm], d11 = p0[c], d12 = p0[cp];
+                    const double d20 = pp[cm], d21 = pp[c], d22 = pp[cp];
+                    md = taps9_fma(d00, d01, d02, d10, d11, d12, d20, d21, d22);
+                    const double cdsq = taps9_fma(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11,
+                                                  d12 * d12, d20 * d20, d21 * d21, d22 * d22);
+                    dms = md * md;
+                    sds = signed_root(cdsq - dms);
+                } else {
+                    md = mu[c];
+                    dms = dm[c];
+                    sds = sd[c];
+                }
+                sum += sim_cell_quick(mr[c], rms[c], srs[c], md, dms, sds, crd);
+                Em = Ec, Mm = Mc;
+                Ec = Ep, Mc = Mp;
             }
-            const double crd = __fma_rn(kW2, Mc, __fma_rn(kW1, (Mm + Mp) + Ec, kW0 * (Em + Ep)));
-            double md, dms, sds;
-            if (c == 0 || c == P - 1) {
-                const int cm = c == 0 ? 0 : c - 1;
-                const double d00 = pm[cm], d01 = pm[c], d02 = pm[cp];
-                const double d10 = p0[cm], d11 = p0[c], d12 = p0[cp];
-                const double d20 = pp[cm], d21 = pp[c], d22 = pp[cp];
-                md = taps9_fma(d00, d01, d02, d10, d11, d12, d20, d21, d22);
-                const double cdsq = taps9_fma(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12,
+        } else {
+            // exact: the operations and order of table_kernel<false> (the
+            // CPU's cell, src/nsim.zig:293-308, and its row-major sum), with
+            // the operands read from the stage
+            double am = qm[0] * pm[0], a0 = q0[0] * p0[0], ap = qp[0] * pp[0];  // column cm
+            double bm = am, b0 = a0, bp = ap;                                   // column c
+#pragma unroll
+            for (int c = 0; c < P; ++c) {
+                const int cp = c + 1 >= P ? P - 1 : c + 1;
+                const double cm_ = qm[cp] * pm[cp], c0 = q0[cp] * p0[cp], cpp = qp[cp] * pp[cp];
+                const double crd = taps9(am, bm, cm_, a0, b0, c0, ap, bp, cpp);
+                double md, dms, sds;
+                if (c == 0 || c == P - 1) {
+                    const int cmi = c == 0 ? 0 : c - 1;
+                    const double d00 = pm[cmi], d01 = pm[c], d02 = pm[cp];
+                    const double d10 = p0[cmi], d11 = p0[c], d12 = p0[cp];
+                    const double d20 = pp[cmi], d21 = pp[c], d22 = pp[cp];
+                    md = taps9(d00, d01, d02, d10, d11, d12, d20, d21, d22);
+                    const double cdsq = taps9(d00 * d00, d01 * d01, d02 * d02, d10 * d10, d11 * d11, d12 * d12,
                                               d20 * d20, d21 * d21, d22 * d22);
-                dms = md * md;
-                sds = signed_root(cdsq - dms);
-            } else {
-                md = mu[c];
-                dms = dm[c];
-                sds = sd[c];
+                    dms = md * md;
+                    sds = cdsq - dms;
+                } else {
+                    md = mu[c];
+                    dms = dm[c];
+                    sds = sd[c];
+                }
+                sum += sim_cell(mr[c], rms[c], srs[c], md, dms, sds, crd);
+                am = bm, a0 = b0, ap = bp;
+                bm = cm_, b0 = c0, bp = cpp;
             }
-            sum += sim_cell_quick(mr[c], rms[c], srs[c], md, dms, sds, crd);
-            Em = Ec, Mm = Mc;
-            Ec = Ep, Mc = Mp;
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncthreads();
@@ -397,32 +432,46 @@ void nsim_init_attributes() {
     cudaFuncSetAttribute(table_kernel<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(table_kernel<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(table_kernel<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(table_fast_kernel<30, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(table_fast_kernel<30, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(table_fast_kernel<20, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(table_fast_kernel<20, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+#define VQB_STAGED_ATTR(F, PP, W) \
+    cudaFuncSetAttribute(table_staged_kernel<F, PP, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    VQB_STAGED_ATTR(true, 30, 128)
+    VQB_STAGED_ATTR(true, 30, 256)
+    VQB_STAGED_ATTR(true, 20, 128)
+    VQB_STAGED_ATTR(true, 20, 256)
+    VQB_STAGED_ATTR(false, 30, 128)
+    VQB_STAGED_ATTR(false, 30, 256)
+    VQB_STAGED_ATTR(false, 20, 128)
+    VQB_STAGED_ATTR(false, 20, 256)
+#undef VQB_STAGED_ATTR
 }
 
 void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s) {
     if (ntasks <= 0) return;
     const size_t smem = (size_t)4 * nb * P * sizeof(double);
-    if (fast && (P == 30 || P == 20) && (width == 128 || width == 256)) {
+    if ((P == 30 || P == 20) && (width == 128 || width == 256)) {
         const size_t staged = (size_t)2 * kStageRows * ((width + P - 1) + P) * sizeof(double);
-#define VQB_TABLE_FAST(PP, W) table_fast_kernel<PP, W><<<ntasks, W, staged, s>>>(d_tasks, nb);
-        if (P == 30) {
-            if (width == 256) {
-                VQB_TABLE_FAST(30, 256)
-            } else {
-                VQB_TABLE_FAST(30, 128)
-            }
+#define VQB_TABLE_STAGED(F, PP, W) table_staged_kernel<F, PP, W><<<ntasks, W, staged, s>>>(d_tasks, nb);
+#define VQB_TABLE_STAGED_P(F)            \
+    if (P == 30) {                       \
+        if (width == 256) {              \
+            VQB_TABLE_STAGED(F, 30, 256) \
+        } else {                         \
+            VQB_TABLE_STAGED(F, 30, 128) \
+        }                                \
+    } else {                             \
+        if (width == 256) {              \
+            VQB_TABLE_STAGED(F, 20, 256) \
+        } else {                         \
+            VQB_TABLE_STAGED(F, 20, 128) \
+        }                                \
+    }
+        if (fast) {
+            VQB_TABLE_STAGED_P(true)
         } else {
-            if (width == 256) {
-                VQB_TABLE_FAST(20, 256)
-            } else {
-                VQB_TABLE_FAST(20, 128)
-            }
+            VQB_TABLE_STAGED_P(false)
         }
-#undef VQB_TABLE_FAST
+#undef VQB_TABLE_STAGED_P
+#undef VQB_TABLE_STAGED
         launch_counter() += 1;
         return;
     }
