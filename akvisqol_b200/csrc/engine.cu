@@ -375,8 +375,14 @@ uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const Rat
     if (opt_.form == kFormF32) {
         int ntiles = 0;
         const void *d_tiles = tiles_of(gammatone_fast_frames_per_cta(), &ntiles);
+        const int C = tuned(kTuneGammatoneFastCtas, opt_.form, nbi, gammatone_fast_ctas_candidates(),
+                            [&](int c) {
+                                launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H,
+                                                      c, st);
+                            },
+                            st);
         if (begin) VQB_CUDA(cudaEventRecord(begin, st));
-        launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, st);
+        launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, C, st);
     } else {
         const int F = tuned(kTuneGammatone, opt_.form, nbi,
                             opt_.form == kFormF64 ? gammatone_f64fma_frames_candidates(nbi)

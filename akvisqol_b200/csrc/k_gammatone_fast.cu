@@ -144,9 +144,11 @@ __device__ inline void filter_tile(const double (*__restrict__ wx)[kRowPad], int
     }
 }
 
-// kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21.
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads, 768 / kThreads) gammatone_fast_kernel(
+// kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21. kCtasPerSm
+// sets the register budget (3: 80 registers at 256 threads; 4: 64, with a
+// few spills), measured by the autotuner.
+template <int kThreads, int kCtasPerSm>
+__global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammatone_fast_kernel(
     const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, const FastBandCoeffs *__restrict__ coeffs,
     int nb, const double *__restrict__ hann, int window, int hop) {
     __shared__ __align__(16) double raw[2][kCtaFrames][kTileS];  // signal samples, frame-major
@@ -373,18 +375,29 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
     }
 }
 
+std::vector<int> gammatone_fast_ctas_candidates() { return {3, 4}; }
+
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                           int nb, const double *d_hann, int window, int hop, cudaStream_t s) {
+                           int nb, const double *d_hann, int window, int hop, int ctas_per_sm, cudaStream_t s) {
     if (ntiles <= 0) return;
     const Tile *t = static_cast<const Tile *>(d_tiles);
-    if (nb > 24)
-        gammatone_fast_kernel<256><<<ntiles, 256, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
-    else if (nb > 16)
-        gammatone_fast_kernel<192><<<ntiles, 192, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
-    else if (nb > 8)
-        gammatone_fast_kernel<128><<<ntiles, 128, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
-    else
-        gammatone_fast_kernel<64><<<ntiles, 64, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop);
+#define VQB_FAST(T, C) gammatone_fast_kernel<T, C><<<ntiles, T, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop)
+#define VQB_FAST_T(T)   \
+    if (ctas_per_sm == 4) \
+        VQB_FAST(T, 4);   \
+    else                  \
+        VQB_FAST(T, 3);
+    if (nb > 24) {
+        VQB_FAST_T(256)
+    } else if (nb > 16) {
+        VQB_FAST_T(192)
+    } else if (nb > 8) {
+        VQB_FAST_T(128)
+    } else {
+        VQB_FAST_T(64)
+    }
+#undef VQB_FAST_T
+#undef VQB_FAST
     launch_counter() += 1;
 }
 

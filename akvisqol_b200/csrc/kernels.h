@@ -132,8 +132,10 @@ void launch_copy_frames(const CopyJob *d_jobs, int njobs, int nb, int max_cols, 
 // k_gammatone_fast.cu (tiles as fill_gammatone_tile writes them)
 int gammatone_fast_frames_per_cta();
 void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, FastBandCoeffs *out);
+// ctas_per_sm: one of gammatone_fast_ctas_candidates() (register budget).
+std::vector<int> gammatone_fast_ctas_candidates();
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                           int nb, const double *d_hann, int window, int hop, cudaStream_t s);
+                           int nb, const double *d_hann, int window, int hop, int ctas_per_sm, cudaStream_t s);
 // f64 FMA form: two frames per thread; tiles of frames_per_cta frames, one
 // of gammatone_f64fma_frames_candidates(nb) (the first is the default).
 std::vector<int> gammatone_f64fma_frames_candidates(int nb);
