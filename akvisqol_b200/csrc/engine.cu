@@ -375,14 +375,16 @@ uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const Rat
     if (opt_.form == kFormF32) {
         int ntiles = 0;
         const void *d_tiles = tiles_of(gammatone_fast_frames_per_cta(), &ntiles);
-        const int C = tuned(kTuneGammatoneFastCtas, opt_.form, nbi, gammatone_fast_ctas_candidates(),
-                            [&](int c) {
-                                launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H,
-                                                      c, st);
-                            },
-                            st);
+        int *queue = arena_.alloc_n<int>(1);  // the persistent form's work counter
+        auto launch = [&](int shape) {
+            if (shape >= 100) launch_zero(queue, sizeof(int), st);
+            launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, shape, queue, st);
+        };
+        static const std::vector<int> all_shapes = gammatone_fast_shapes();
+        const int shape =
+            tuned(kTuneGammatoneFastCtas, opt_.form, nbi, gammatone_fast_shape_candidates(), launch, st, &all_shapes);
         if (begin) VQB_CUDA(cudaEventRecord(begin, st));
-        launch_gammatone_fast(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, C, st);
+        launch(shape);
     } else {
         const int F = tuned(kTuneGammatone, opt_.form, nbi,
                             opt_.form == kFormF64 ? gammatone_f64fma_frames_candidates(nbi)
@@ -418,7 +420,14 @@ bool autotune_enabled() {
 }  // namespace
 
 int Engine::tuned(int kernel, int a, int b, const std::vector<int> &candidates,
-                  const std::function<void(int)> &launch, cudaStream_t st) {
+                  const std::function<void(int)> &launch, cudaStream_t st, const std::vector<int> *allowed) {
+    // VISQOL_TUNE_<kernel>=<choice> fixes a kernel class's shape (one of its
+    // candidates), e.g. to check that every shape gives the same results.
+    if (const char *env = std::getenv(("VISQOL_TUNE_" + std::to_string(kernel)).c_str())) {
+        const int forced = std::atoi(env);
+        const std::vector<int> &ok = allowed ? *allowed : candidates;
+        if (std::find(ok.begin(), ok.end(), forced) != ok.end()) return forced;
+    }
     if (!autotune_enabled() || candidates.size() < 2) return candidates.at(0);
     const auto key = std::make_tuple(device_, kernel, a, b);
     {

@@ -177,8 +177,10 @@ private:
     // caller's jobs at first use per device (launch(c) launches them with
     // shape c on st), then reused; candidates[0] when autotuning is off.
     enum TuneKernel { kTuneGammatone = 0, kTuneTable = 1, kTuneLagColumns = 2, kTuneGammatoneFastCtas = 3 };
+    // VISQOL_TUNE_<kernel> may fix the shape to one of `allowed` (default:
+    // the candidates).
     int tuned(int kernel, int a, int b, const std::vector<int> &candidates, const std::function<void(int)> &launch,
-              cudaStream_t st);
+              cudaStream_t st, const std::vector<int> *allowed = nullptr);
     // Gammatone spectrograms of the jobs in this engine's form on stream st;
     // returns the RMS count.
     uint64_t launch_spectrograms(const std::vector<SpecJob> &jobs, const RateCache &rc, cudaStream_t st,

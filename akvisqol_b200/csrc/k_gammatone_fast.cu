@@ -38,6 +38,8 @@
 // shared-memory word (a broadcast), and every band of a warp takes the same
 // form (the host groups bands by 8). A CTA holds ceil(nb/8) band groups x 2
 // frame blocks of 8 frames.
+#include <algorithm>
+
 #include "device.cuh"
 #include "kernels.h"
 
@@ -144,16 +146,14 @@ __device__ inline void filter_tile(const double (*__restrict__ wx)[kRowPad], int
     }
 }
 
-// kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21. kCtasPerSm
-// sets the register budget (3: 80 registers at 256 threads; 4: 64, with a
-// few spills), measured by the autotuner.
-template <int kThreads, int kCtasPerSm>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammatone_fast_kernel(
-    const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, const FastBandCoeffs *__restrict__ coeffs,
-    int nb, const double *__restrict__ hann, int window, int hop) {
-    __shared__ __align__(16) double raw[2][kCtaFrames][kTileS];  // signal samples, frame-major
-    __shared__ __align__(16) double wx[2][kTileS][kRowPad];      // windowed, sample-major
-    const Tile tile = tiles[blockIdx.x];
+// One tile (16 frames x all bands of one job) of the FP32 form. raw, wx:
+// the CTA's shared-memory staging (raw[2][16][kTileS] signal samples,
+// frame-major; wx[2][kTileS][kRowPad] windowed samples, sample-major).
+template <int kThreads>
+__device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__restrict__ jobs,
+                                          const FastBandCoeffs *__restrict__ coeffs, int nb,
+                                          const double *__restrict__ hann, int window, int hop,
+                                          double (*raw)[kCtaFrames][kTileS], double (*wx)[kTileS][kRowPad]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int groups = (nb + 7) >> 3;
     const int g = warp % groups, fblock = warp / groups;
@@ -224,11 +224,39 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammato
         }
         buf ^= 1;
     }
-    if (band_raw >= nb || f >= job.nf) return;
-    const double inv_n = 1.0 / (double)window;
-    double *out = job.out + (int64_t)band * job.nf;
-    out[f] = sqrt(acc_a * inv_n) * k.post64;
-    if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post64;
+    if (band_raw < nb && f < job.nf) {
+        const double inv_n = 1.0 / (double)window;
+        double *out = job.out + (int64_t)band * job.nf;
+        out[f] = sqrt(acc_a * inv_n) * k.post64;
+        if (f + 1 < job.nf) out[f + 1] = sqrt(acc_b * inv_n) * k.post64;
+    }
+}
+
+// kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21. kCtasPerSm
+// sets the register budget (3: 80 registers at 256 threads; 4: 64, with a
+// few spills). kPersistent: a grid of kCtasPerSm CTAs per SM takes tiles
+// from a device-side work queue (an atomic counter over the tile list, zero
+// at launch) instead of one CTA per tile. Both choices are measured by the
+// autotuner; every tile is computed the same either way.
+template <int kThreads, int kCtasPerSm, bool kPersistent>
+__global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammatone_fast_kernel(
+    const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, int ntiles, int *__restrict__ queue,
+    const FastBandCoeffs *__restrict__ coeffs, int nb, const double *__restrict__ hann, int window, int hop) {
+    __shared__ __align__(16) double raw[2][kCtaFrames][kTileS];
+    __shared__ __align__(16) double wx[2][kTileS][kRowPad];
+    if constexpr (!kPersistent) {
+        fast_tile<kThreads>(tiles[blockIdx.x], jobs, coeffs, nb, hann, window, hop, raw, wx);
+    } else {
+        __shared__ int next;
+        for (;;) {
+            if (threadIdx.x == 0) next = atomicAdd(queue, 1);
+            __syncthreads();
+            const int ti = next;
+            if (ti >= ntiles) return;  // the same for the whole CTA
+            fast_tile<kThreads>(tiles[ti], jobs, coeffs, nb, hann, window, hop, raw, wx);
+            __syncthreads();  // staging buffers and `next` free for the next tile
+        }
+    }
 }
 
 // Samples of a frame: straight loads when the whole window lies inside the
@@ -375,18 +403,45 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
     }
 }
 
-std::vector<int> gammatone_fast_ctas_candidates() { return {3, 4}; }
+// Launch shapes: CTAs per SM (register budget) + 100 for the persistent
+// work-queue form. The autotuner measures the first two; the persistent
+// shapes measured ~4.5% slower inside the four-lane batch pipeline (their
+// resident CTAs hold SMs the other lanes' kernels would take) and are
+// selected only by VISQOL_TUNE_3.
+std::vector<int> gammatone_fast_shape_candidates() { return {3, 4}; }
+std::vector<int> gammatone_fast_shapes() { return {3, 4, 103, 104}; }
+
+namespace {
+int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+}  // namespace
 
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                           int nb, const double *d_hann, int window, int hop, int ctas_per_sm, cudaStream_t s) {
+                           int nb, const double *d_hann, int window, int hop, int shape, int *d_queue,
+                           cudaStream_t s) {
     if (ntiles <= 0) return;
     const Tile *t = static_cast<const Tile *>(d_tiles);
-#define VQB_FAST(T, C) gammatone_fast_kernel<T, C><<<ntiles, T, 0, s>>>(d_jobs, t, d_coeffs, nb, d_hann, window, hop)
-#define VQB_FAST_T(T)   \
-    if (ctas_per_sm == 4) \
-        VQB_FAST(T, 4);   \
-    else                  \
-        VQB_FAST(T, 3);
+    const int ctas = shape % 100;
+    const bool persistent = shape >= 100 && d_queue;
+    const int grid = persistent ? std::min(ntiles, sm_count() * ctas) : ntiles;
+#define VQB_FAST(T, C, P)                                                                                    \
+    gammatone_fast_kernel<T, C, P><<<grid, T, 0, s>>>(d_jobs, t, ntiles, d_queue, d_coeffs, nb, d_hann, window, \
+                                                      hop)
+#define VQB_FAST_T(T)                    \
+    if (persistent) {                    \
+        if (ctas == 4)                   \
+            VQB_FAST(T, 4, true);        \
+        else                             \
+            VQB_FAST(T, 3, true);        \
+    } else if (ctas == 4) {              \
+        VQB_FAST(T, 4, false);           \
+    } else {                             \
+        VQB_FAST(T, 3, false);           \
+    }
     if (nb > 24) {
         VQB_FAST_T(256)
     } else if (nb > 16) {

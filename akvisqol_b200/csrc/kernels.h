@@ -132,10 +132,14 @@ void launch_copy_frames(const CopyJob *d_jobs, int njobs, int nb, int max_cols, 
 // k_gammatone_fast.cu (tiles as fill_gammatone_tile writes them)
 int gammatone_fast_frames_per_cta();
 void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, FastBandCoeffs *out);
-// ctas_per_sm: one of gammatone_fast_ctas_candidates() (register budget).
-std::vector<int> gammatone_fast_ctas_candidates();
+// shape: one of gammatone_fast_shape_candidates(): CTAs per SM (register
+// budget), plus 100 for the persistent form, which takes its tiles from a
+// work queue: d_queue, one int that is zero when the launch starts.
+std::vector<int> gammatone_fast_shape_candidates();  // measured by the autotuner
+std::vector<int> gammatone_fast_shapes();            // all valid shapes
 void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
-                           int nb, const double *d_hann, int window, int hop, int ctas_per_sm, cudaStream_t s);
+                           int nb, const double *d_hann, int window, int hop, int shape, int *d_queue,
+                           cudaStream_t s);
 // f64 FMA form: two frames per thread; tiles of frames_per_cta frames, one
 // of gammatone_f64fma_frames_candidates(nb) (the first is the default).
 std::vector<int> gammatone_f64fma_frames_candidates(int nb);

@@ -166,7 +166,8 @@ int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double 
 /* Launch shapes the autotuner has chosen in this process: *n_rows rows of
  * {device, kernel (0 gammatone frames per CTA, 1 NSIM-table offsets per
  * CTA, 2 lag-search column passes: 0 shared-memory tiles, 1 registers, 3
- * FP32-form gammatone CTAs per SM, i.e. its register budget),
+ * FP32-form gammatone: CTAs per SM (its register budget), + 100 for the
+ * persistent form that takes its tiles from a device-side work queue),
  * variant a (form / cell arithmetic / log2 transform size), variant b
  * (bands / raw signals), choice},
  * written to rows up to max_rows. Each kernel class is measured on its

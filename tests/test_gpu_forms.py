@@ -80,3 +80,22 @@ def test_batch_equals_single(native, contexts, form):
         assert code == code1 == 0
         assert res["moslqo"] == res1["moslqo"]
         assert np.array_equal(res["fvnsim"], res1["fvnsim"])
+
+
+@pytest.mark.parametrize("shape", ["3", "4", "103", "104"])
+def test_fast_gammatone_shapes_agree(native, monkeypatch, shape):
+    """Every launch shape of the FP32-form gammatone kernel (register budget of
+    3 or 4 CTAs per SM; one CTA per tile, or a persistent grid taking tiles
+    from a device-side work queue) gives the same bits."""
+    from akvisqol_b200 import synth
+    pairs = synth.audio_batch(5, seed0=synth.SEED_BASE + 700, min_s=2.0, max_s=6.0)
+    refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
+    ctx = native.Context(mode=native.MODE_AUDIO, precision="fast")
+    monkeypatch.setenv("VISQOL_TUNE_3", "3")
+    base = ctx.measure_batch_traced(refs, degs, 48000)
+    monkeypatch.setenv("VISQOL_TUNE_3", shape)
+    got = ctx.measure_batch_traced(refs, degs, 48000)
+    for (c0, r0, _), (c1, r1, _) in zip(base, got):
+        assert c0 == c1 == 0
+        assert r0["moslqo"] == r1["moslqo"]
+        assert np.array_equal(r0["fvnsim"], r1["fvnsim"])
