@@ -6,6 +6,8 @@
 // files grouped by sample rate. The engine behind it is the GPU pipeline;
 // there is no CPU fallback.
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,8 +15,10 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -28,12 +32,13 @@
 using vqb::Error;
 
 // A context owns one or more lanes: engines with their own streams and
-// memory on the same GPU (VISQOL_GPU_LANES, default 4; the reference's GPU
+// memory on the same GPU (VISQOL_GPU_LANES, default 6; the reference's GPU
 // engine runs two, src/gpu/engine.zig:551-591). A batch is split across the
-// lanes by signal length and the lanes run concurrently from host threads,
-// so one lane's serial phases, host planning and uploads overlap another's
-// kernels. On one B200, 4 lanes score a 128-pair batch of 10 s 48 kHz host
-// signals ~5% faster than 2 (the device-resident rate is the same).
+// lanes and the lanes run concurrently from host threads, so one lane's
+// serial phases, host planning and uploads overlap another's kernels. On one
+// B200 the device-resident rate of a 128-pair batch of 10 s 48 kHz pairs is
+// the same for 2, 4 and 6 lanes; with host inputs, 6 lanes score it ~5%
+// faster than 4 (the uploads hide behind more concurrent chunks).
 // References prepared once for many degraded signals (visqol_b200_prepare).
 struct visqol_b200_prepared {
     int device = 0;
@@ -42,11 +47,32 @@ struct visqol_b200_prepared {
     std::vector<std::unique_ptr<vqb::PreparedRef>> refs;
 };
 
+// Device staging for host-input batches scored through the shared chunk
+// queue (run_lanes_queued): a grow-only buffer for a whole batch's signals,
+// a copy stream and one event per chunk (created on first use).
+struct HostStaging {
+    int device = 0;
+    double *buf = nullptr;
+    size_t bytes = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t piece = nullptr;
+    std::vector<cudaEvent_t> chunk_done;
+    ~HostStaging() {
+        cudaSetDevice(device);
+        if (copy) cudaStreamSynchronize(copy);
+        for (auto e : chunk_done) cudaEventDestroy(e);
+        if (piece) cudaEventDestroy(piece);
+        if (copy) cudaStreamDestroy(copy);
+        cudaFree(buf);
+    }
+};
+
 struct visqol_ctx {
     vqb::Options opt;
     std::shared_ptr<const vqb::host::Svr> svr;
     std::vector<std::unique_ptr<vqb::Engine>> lanes;
     vqb::Timing timing;
+    std::unique_ptr<HostStaging> staging;
 };
 
 namespace {
@@ -141,6 +167,198 @@ int device_count() {
     return n;
 }
 
+// Whether a batch of this kind (device, form, mode, sample rate) has run in
+// this process. The first one scores its first share on one lane alone, so
+// that the autotuner's measurements (made on that first batch's jobs) are
+// not timed beside other lanes' kernels; the rest then runs concurrently.
+bool first_of_its_kind(const visqol_ctx *c, uint32_t sample_rate) {
+    static std::mutex mu;
+    static std::set<std::tuple<int, int, bool, uint32_t>> seen;
+    const auto key = std::make_tuple(c->lanes[0]->device(), (int)c->opt.form, c->opt.speech, sample_rate);
+    std::lock_guard<std::mutex> lock(mu);
+    return seen.insert(key).second;
+}
+
+// Host-input batches through all lanes at once: the signals go up in chunks
+// of consecutive pairs, in order, on a copy stream of their own (one copy in
+// flight, so the lanes' own small uploads never queue behind a whole chunk),
+// and the lanes take chunks from a shared queue as they free up, each
+// waiting on its chunk's upload. The GPU starts scoring when the first chunk
+// has landed, the transfer of the rest overlaps the scoring, and every chunk
+// is scored as one batch of a reasonable size. Returns false (nothing done)
+// when the batch is too small to split or too large for one staging buffer;
+// the caller then takes the per-lane path.
+bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,
+                      const double *const *degs, const size_t *deg_lens, uint32_t sample_rate,
+                      std::vector<vqb::PairOutcome> &res, const vqb::PreparedRef *const *prepared) {
+    const size_t L = c->lanes.size();
+    auto up = [](size_t len) { return (len * sizeof(double) + 255) & ~size_t(255); };
+    std::vector<size_t> ref_off(n, SIZE_MAX), deg_off(n, SIZE_MAX);
+    size_t total = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (!(prepared && prepared[i]) && refs[i]) ref_off[i] = total, total += up(ref_lens[i]);
+        if (degs[i]) deg_off[i] = total, total += up(deg_lens[i]);
+    }
+    const size_t K = std::min(n, 2 * L);
+    size_t min_bytes = size_t(64) << 20;  // VISQOL_STREAMED_MIN_BYTES overrides, as for the per-lane path
+    if (const char *env = std::getenv("VISQOL_STREAMED_MIN_BYTES")) min_bytes = (size_t)std::strtoull(env, nullptr, 10);
+    if (L < 2 || K < 2 || total < min_bytes || total > (size_t(16) << 30)) return false;
+    const int device = c->lanes[0]->device();
+    VQB_CUDA(cudaSetDevice(device));
+    if (!c->staging) {
+        c->staging = std::make_unique<HostStaging>();
+        c->staging->device = device;
+        VQB_CUDA(cudaStreamCreateWithFlags(&c->staging->copy, cudaStreamNonBlocking));
+        VQB_CUDA(cudaEventCreateWithFlags(&c->staging->piece, cudaEventDisableTiming));
+    }
+    HostStaging &st = *c->staging;
+    if (st.bytes < total) {
+        VQB_CUDA(cudaStreamSynchronize(st.copy));
+        if (st.buf) VQB_CUDA(cudaFree(st.buf));
+        st.buf = nullptr;
+        st.bytes = 0;
+        VQB_CUDA(cudaMalloc(&st.buf, total));
+        st.bytes = total;
+    }
+    while (st.chunk_done.size() < K) {
+        cudaEvent_t e;
+        VQB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        st.chunk_done.push_back(e);
+    }
+    // chunks of about equal bytes, consecutive pairs
+    std::vector<size_t> bounds{0};
+    {
+        size_t acc = 0;
+        for (size_t i = 0; i < n && bounds.size() < K; ++i) {
+            acc += (ref_off[i] != SIZE_MAX ? up(ref_lens[i]) : 0) + (deg_off[i] != SIZE_MAX ? up(deg_lens[i]) : 0);
+            if (acc * K >= total * bounds.size() && i + 1 < n) bounds.push_back(i + 1);
+        }
+        bounds.push_back(n);
+    }
+    const size_t nk = bounds.size() - 1;
+    char *base = reinterpret_cast<char *>(st.buf);
+    std::vector<const double *> d_ref(n, nullptr), d_deg(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        if (ref_off[i] != SIZE_MAX) d_ref[i] = reinterpret_cast<const double *>(base + ref_off[i]);
+        if (deg_off[i] != SIZE_MAX) d_deg[i] = reinterpret_cast<const double *>(base + deg_off[i]);
+    }
+    // uploader: chunk k's copies, then its event; `recorded` tells the lanes
+    // (host side) that the event they will wait on has been recorded
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t recorded = 0;
+    bool failed = false;
+    std::exception_ptr upload_error;
+    std::thread uploader([&] {
+        try {
+            VQB_CUDA(cudaSetDevice(device));
+            size_t copies = 0;
+            auto copy = [&](const double *dst, const double *src, size_t len) {
+                if (!len) return;
+                if (copies++) VQB_CUDA(cudaEventSynchronize(st.piece));
+                VQB_CUDA(cudaMemcpyAsync(const_cast<double *>(dst), src, len * sizeof(double), cudaMemcpyHostToDevice,
+                                         st.copy));
+                VQB_CUDA(cudaEventRecord(st.piece, st.copy));
+            };
+            for (size_t k = 0; k < nk; ++k) {
+                for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) {
+                    if (d_ref[i]) copy(d_ref[i], refs[i], ref_lens[i]);
+                    if (d_deg[i]) copy(d_deg[i], degs[i], deg_lens[i]);
+                }
+                VQB_CUDA(cudaEventRecord(st.chunk_done[k], st.copy));
+                std::lock_guard<std::mutex> lock(mu);
+                recorded = k + 1;
+                cv.notify_all();
+            }
+        } catch (...) {
+            upload_error = std::current_exception();
+            std::lock_guard<std::mutex> lock(mu);
+            failed = true;
+            cv.notify_all();
+        }
+    });
+    std::atomic<size_t> next{0};
+    std::vector<std::exception_ptr> errs(L);
+    std::vector<vqb::Timing> lane_t(L);
+    const bool alone_first = first_of_its_kind(c, sample_rate);
+    // Lane l scores chunk k; false when the upload failed (reported below).
+    auto score_chunk = [&](size_t l, size_t k) -> bool {
+        try {
+            vqb::Engine &e = *c->lanes[l];
+            std::vector<vqb::PairOutcome> part;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                cv.wait(lock, [&] { return recorded > k || failed; });
+                if (recorded <= k) return false;
+            }
+            VQB_CUDA(cudaStreamWaitEvent(e.stream(), st.chunk_done[k], 0));
+            const size_t b0 = bounds[k], m = bounds[k + 1] - b0;
+            e.measure_batch(m, d_ref.data() + b0, ref_lens + b0, d_deg.data() + b0, deg_lens + b0, sample_rate,
+                            true, part, prepared ? prepared + b0 : nullptr, refs + b0);
+            for (size_t j = 0; j < m; ++j) res[b0 + j] = std::move(part[j]);
+            const vqb::Timing &t = e.last_timing();
+            vqb::Timing &a = lane_t[l];
+            a.total_ms += t.total_ms;
+            a.lag_ms += t.lag_ms;
+            a.spectrogram_ms += t.spectrogram_ms;
+            a.prep_ms += t.prep_ms;
+            a.nsim_ms += t.nsim_ms;
+            a.realign_ms += t.realign_ms;
+            a.gammatone_kernel_ms += t.gammatone_kernel_ms;
+            a.gammatone_launches += t.gammatone_launches;
+            a.gammatone_rms += t.gammatone_rms;
+            a.gammatone_window = std::max(a.gammatone_window, t.gammatone_window);
+            a.kernel_launches += t.kernel_launches;
+            a.h2d_bytes += t.h2d_bytes;
+            a.d2h_bytes += t.d2h_bytes;
+            a.host_syncs += t.host_syncs;
+        } catch (...) {
+            if (!errs[l]) errs[l] = std::current_exception();
+            return false;
+        }
+        return true;
+    };
+    auto work = [&](size_t l) {
+        for (size_t k = next++; k < nk; k = next++)
+            if (!score_chunk(l, k)) return;
+    };
+    std::vector<std::thread> threads;
+    if (alone_first) {
+        // lane 0 scores chunk 0 alone (the autotuner measures there), then
+        // all lanes share the remaining chunks
+        next = 1;
+        score_chunk(0, 0);
+    }
+    for (size_t l = 1; l < L; ++l) threads.emplace_back(work, l);
+    work(0);
+    for (auto &t : threads) t.join();
+    uploader.join();
+    if (upload_error) std::rethrow_exception(upload_error);
+    for (auto &e : errs)
+        if (e) std::rethrow_exception(e);
+    vqb::Timing t{};
+    for (const vqb::Timing &x : lane_t) {
+        t.total_ms = std::max(t.total_ms, x.total_ms);
+        t.lag_ms = std::max(t.lag_ms, x.lag_ms);
+        t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
+        t.prep_ms = std::max(t.prep_ms, x.prep_ms);
+        t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
+        t.realign_ms = std::max(t.realign_ms, x.realign_ms);
+        t.gammatone_kernel_ms += x.gammatone_kernel_ms;
+        t.gammatone_launches += x.gammatone_launches;
+        t.gammatone_rms += x.gammatone_rms;
+        t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
+        t.kernel_launches += x.kernel_launches;
+        t.h2d_bytes += x.h2d_bytes;
+        t.d2h_bytes += x.d2h_bytes;
+        t.host_syncs += x.host_syncs;
+    }
+    for (size_t i = 0; i < n; ++i)
+        t.h2d_bytes += (d_ref[i] ? ref_lens[i] : 0) * sizeof(double) + (d_deg[i] ? deg_lens[i] : 0) * sizeof(double);
+    c->timing = t;
+    return true;
+}
+
 // The batch across the context's lanes: pairs dealt longest-first to the
 // least-loaded lane, lanes run concurrently, outcomes gathered back in order.
 void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
@@ -148,8 +366,10 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
                const vqb::PreparedRef *const *prepared = nullptr) {
     const size_t L = std::min(c->lanes.size(), std::max<size_t>(1, n));
     res.assign(n, vqb::PairOutcome{});
-    // Host inputs: each lane overlaps its uploads with its scoring.
+    // Host inputs: uploads overlap scoring, through the shared chunk queue
+    // when the batch splits, else lane by lane.
     const bool streamed = !device_inputs && vqb::env_streamed_uploads();
+    if (streamed && run_lanes_queued(c, n, refs, ref_lens, degs, deg_lens, sample_rate, res, prepared)) return;
     auto measure = [&](vqb::Engine &e, size_t m, const double *const *r, const size_t *rl, const double *const *d,
                        const size_t *dl, std::vector<vqb::PairOutcome> &o, const vqb::PreparedRef *const *pr) {
         if (streamed)
@@ -176,6 +396,7 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
     }
     std::vector<std::vector<vqb::PairOutcome>> lane_out(L);
     std::vector<std::exception_ptr> errs(L);
+    const bool alone_first = first_of_its_kind(c, sample_rate);
     auto work = [&](size_t l) {
         try {
             const auto &ix = part[l];
@@ -193,8 +414,11 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
         }
     };
     std::vector<std::thread> threads;
+    // the first batch of its kind: lane 0's share alone (the autotuner
+    // measures there), then the other lanes
+    if (alone_first) work(0);
     for (size_t l = 1; l < L; ++l) threads.emplace_back(work, l);
-    work(0);
+    if (!alone_first) work(0);
     for (auto &t : threads) t.join();
     for (auto &e : errs)
         if (e) std::rethrow_exception(e);
@@ -366,7 +590,7 @@ int visqol_create(const visqol_options *in, visqol_ctx **out) {
         if (int rc = vqb::engine_options(o, &c->opt, &c->svr, &lattice, &msg)) return fail(rc, msg);
         int dev = 0;
         if (int rc = vqb::context_device(&dev, &msg)) return fail(rc, msg);
-        const int lanes = vqb::env_lanes(4);
+        const int lanes = vqb::env_lanes(6);
         for (int l = 0; l < lanes; ++l)
             c->lanes.push_back(std::make_unique<vqb::Engine>(dev, c->opt, c->svr, lattice));
     } catch (const Error &e) {

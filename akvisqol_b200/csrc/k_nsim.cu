@@ -423,7 +423,12 @@ void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaS
 
 int table_offsets_per_cta() { return kTableThreads; }
 
-std::vector<int> table_width_candidates() { return {128, 64, 256}; }
+std::vector<int> table_width_candidates(int P) {
+    // widths the staged kernels have for the audio and speech patch widths;
+    // 64 would fall back to the unstaged kernel
+    if (P == 30 || P == 20) return {128, 256};
+    return {128, 64, 256};
+}
 
 void nsim_init_attributes() {
     cudaFuncSetAttribute(table_kernel<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -159,9 +159,9 @@ void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cuda
 void launch_ref_terms(const RefTermsJob *d_jobs, int njobs, int nb, int P, cudaStream_t s);
 int table_offsets_per_cta();
 // fast: the fast forms' cell arithmetic (FMA, one division per cell);
-// width: offsets per CTA, one of table_width_candidates() (the first is the
+// width: offsets per CTA, one of table_width_candidates(P) (the first is the
 // default); tasks must be built with the same width.
-std::vector<int> table_width_candidates();
+std::vector<int> table_width_candidates(int P);
 void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s);
 void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s);
 

@@ -326,6 +326,34 @@ class Context:
         lib.visqol_measure_files_batch(self._handle, n, refs, degs, num_threads, outs, status)
         return _collect(outs, status, n)
 
+    def measure_batch_scores(self, refs, degs, sample_rate: int, device_inputs: bool = False,
+                             ref_lens=None, deg_lens=None):
+        """Batch without traces: a list of ``(code, MOS or None)`` (the
+        results are freed here)."""
+        n = len(refs)
+        if device_inputs:
+            rp = (c_void_p * n)(*[int(a) for a in refs])
+            dp = (c_void_p * n)(*[int(a) for a in degs])
+            rl = (c_size_t * n)(*ref_lens)
+            dl = (c_size_t * n)(*deg_lens)
+        else:
+            rp = (c_void_p * n)(*[a.ctypes.data for a in refs])
+            dp = (c_void_p * n)(*[a.ctypes.data for a in degs])
+            rl = (c_size_t * n)(*[a.size for a in refs])
+            dl = (c_size_t * n)(*[a.size for a in degs])
+        outs = (POINTER(Result) * n)()
+        status = (c_int32 * n)()
+        lib.visqol_b200_measure_batch(self._handle, n, rp, rl, dp, dl, sample_rate,
+                                      DEVICE_INPUTS if device_inputs else 0, outs, status, None)
+        res = []
+        for i in range(n):
+            if status[i] == OK:
+                res.append((OK, outs[i].contents.moslqo))
+                free(outs[i])
+            else:
+                res.append((status[i], None))
+        return res
+
     def measure_batch_traced(self, refs, degs, sample_rate: int, device_inputs: bool = False,
                              ref_lens=None, deg_lens=None):
         """Batch with per-pair traces. Host arrays, or device addresses (ints)

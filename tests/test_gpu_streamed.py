@@ -1,9 +1,11 @@
-"""Host-input batches whose uploads overlap scoring (chunked uploads on a
-copy stream into two device slots) give exactly the results of the same
-pairs uploaded all at once, and of the pairs given as device inputs: every
-pair's result depends only on its own signals, so chunking changes nothing
-but the timing. The byte bound below which batches take the direct path is
-lowered here so that small batches split into several chunks."""
+"""Host-input batches whose uploads overlap scoring (chunks uploaded on a
+copy stream while earlier chunks are scored: lanes sharing a queue of
+chunks, or one lane chunking its own batch into two device slots) give
+exactly the results of the same pairs uploaded all at once, and of the pairs
+given as device inputs: every pair's result depends only on its own signals,
+so chunking changes nothing but the timing. The byte bound below which
+batches take the direct path is lowered here so that small batches split
+into several chunks."""
 
 import numpy as np
 import pytest
@@ -53,14 +55,18 @@ def _check(monkeypatch, ctx, refs, degs, sr):
     return streamed
 
 
+@pytest.mark.parametrize("lanes", ["1", "4"])
 @pytest.mark.parametrize("precision", ["exact", "fast"])
-def test_streamed_audio_uneven(native, monkeypatch, precision):
+def test_streamed_audio_uneven(native, monkeypatch, precision, lanes):
+    """One lane: the lane chunks its own batch (Engine::measure_batch_streamed);
+    four lanes: the lanes share a queue of chunks uploaded in order."""
     from akvisqol_b200 import synth
     pairs = synth.audio_batch(9, seed0=synth.SEED_BASE + 300, min_s=2.0, max_s=7.0)
     refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
     # one pair too short to score: its error code comes back unchanged
     refs.insert(4, refs[4][:1000].copy())
     degs.insert(4, degs[4][:1000].copy())
+    monkeypatch.setenv("VISQOL_GPU_LANES", lanes)
     ctx = native.Context(mode=native.MODE_AUDIO, precision=precision)
     got = _check(monkeypatch, ctx, refs, degs, 48000)
     assert got[4][0] != 0
