@@ -55,7 +55,7 @@ WORKLOAD = "audio-mode pairs, 10 s at 48 kHz (480,000 samples; degraded 481,776)
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--batch", type=int, default=128)
     p.add_argument("--seconds", type=float, default=10.0)
@@ -108,7 +108,7 @@ def make_pairs(count: int, seconds: float, seed0: int):
 
 
 class Clocks:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
+    """nvidia-smi samples every 100 ms while the timed region runs."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -121,7 +121,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
