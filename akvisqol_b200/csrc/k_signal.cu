@@ -79,10 +79,19 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
         const double *c0 = tiles + buf * 2 * kTile, *c1 = c0 + kTile;
         const int64_t left = n - base;
         if (left >= kTile) {
-#pragma unroll 32
-            for (int e = 0; e < kTile; ++e) {
-                acc0 += c0[e];
-                if (KIND == kSumAndEnergy) acc1 += c1[e];
+            // addends two at a time (16-byte broadcast loads), in index order
+            const double2 *d0 = reinterpret_cast<const double2 *>(c0);
+            const double2 *d1 = reinterpret_cast<const double2 *>(c1);
+#pragma unroll 16
+            for (int e = 0; e < kTile / 2; ++e) {
+                const double2 a = d0[e];
+                acc0 += a.x;
+                acc0 += a.y;
+                if (KIND == kSumAndEnergy) {
+                    const double2 b = d1[e];
+                    acc1 += b.x;
+                    acc1 += b.y;
+                }
             }
         } else {
             for (int e = 0; e < (int)left; ++e) {
@@ -98,7 +107,7 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
 
 template <int KIND>
 __global__ void __launch_bounds__(32 * kSerialWarps) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
-    __shared__ double tiles[kSerialWarps][4 * kTile];
+    __shared__ __align__(16) double tiles[kSerialWarps][4 * kTile];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -132,7 +141,7 @@ struct AlignedEnergyArgs {
 
 __global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs,
                                                                             int njobs) {
-    __shared__ double tiles[kSerialWarps][4 * kTile];
+    __shared__ __align__(16) double tiles[kSerialWarps][4 * kTile];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
