@@ -390,13 +390,35 @@ uint64_t Engine::launch_spectrograms(const std::vector<SpecJob> &jobs, const Rat
                             opt_.form == kFormF64 ? gammatone_f64fma_frames_candidates(nbi)
                                                   : gammatone_frames_candidates(nbi),
                             launch_frames, st);
-        int ntiles = 0;
-        const void *d_tiles = tiles_of(F, &ntiles);
-        if (begin) VQB_CUDA(cudaEventRecord(begin, st));
-        if (opt_.form == kFormF64)
-            launch_gammatone_f64fma(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, nbi, rc.d_hann, W, H, F, st);
-        else
+        if (opt_.form == kFormF64) {
+            // the FP64-FMA kernel at that shape, or the same form on the FP32
+            // kernel's staged tiles (same bits); tile lists uploaded on first use
+            int ntiles[2] = {0, 0};
+            const void *d_tiles[2] = {nullptr, nullptr};
+            auto ensure_tiles = [&](int staged) {
+                if (!d_tiles[staged])
+                    d_tiles[staged] = tiles_of(staged ? gammatone_fast_frames_per_cta() : F, &ntiles[staged]);
+            };
+            auto launch = [&](int staged) {
+                ensure_tiles(staged);
+                if (staged)
+                    launch_gammatone_f64_staged(d_jobs, d_tiles[1], ntiles[1], rc.d_fast_coeffs, nbi, rc.d_hann, W, H,
+                                                st);
+                else
+                    launch_gammatone_f64fma(d_jobs, d_tiles[0], ntiles[0], rc.d_fast_coeffs, nbi, rc.d_hann, W, H, F,
+                                            st);
+            };
+            const int staged =
+                tuned(kTuneGammatoneF64Staged, opt_.form, nbi, gammatone_f64_staged_candidates(), launch, st);
+            ensure_tiles(staged);
+            if (begin) VQB_CUDA(cudaEventRecord(begin, st));
+            launch(staged);
+        } else {
+            int ntiles = 0;
+            const void *d_tiles = tiles_of(F, &ntiles);
+            if (begin) VQB_CUDA(cudaEventRecord(begin, st));
             launch_gammatone(d_jobs, d_tiles, ntiles, rc.d_coeffs, nbi, rc.d_hann, W, H, F, st);
+        }
     }
     if (end) VQB_CUDA(cudaEventRecord(end, st));
     return rms;

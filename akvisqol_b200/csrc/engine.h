@@ -176,7 +176,13 @@ private:
     // The launch shape for a kernel class among candidates: measured on the
     // caller's jobs at first use per device (launch(c) launches them with
     // shape c on st), then reused; candidates[0] when autotuning is off.
-    enum TuneKernel { kTuneGammatone = 0, kTuneTable = 1, kTuneLagColumns = 2, kTuneGammatoneFastCtas = 3 };
+    enum TuneKernel {
+        kTuneGammatone = 0,
+        kTuneTable = 1,
+        kTuneLagColumns = 2,
+        kTuneGammatoneFastCtas = 3,
+        kTuneGammatoneF64Staged = 4
+    };
     // VISQOL_TUNE_<kernel> may fix the shape to one of `allowed` (default:
     // the candidates).
     int tuned(int kernel, int a, int b, const std::vector<int> &candidates, const std::function<void(int)> &launch,

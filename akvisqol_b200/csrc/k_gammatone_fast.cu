@@ -113,6 +113,32 @@ struct F64Pair {
     }
 };
 
+// The FP64-FMA form's four stages of one frame, direct form I with
+// unit-leading numerators, and its sum of squares. Both kernels of that form
+// run two frames per thread (the second hop samples later): two independent
+// recurrences give each warp twice the FP64 work between dependent steps.
+struct Cascade64 {
+    double xp = 0.0, y1a = 0.0, y2a = 0.0, y1b = 0.0, y2b = 0.0, y1c = 0.0, y2c = 0.0, y1d = 0.0, y2d = 0.0;
+    double acc = 0.0;
+    __device__ inline void step(double x, double b0, double b1, double b2, double b3, double nd1, double nd2) {
+        // stage k input v, previous input = stage k-1's previous output
+        const double ya = __fma_rn(nd1, y1a, __fma_rn(nd2, y2a, __fma_rn(b0, xp, x)));
+        const double yb = __fma_rn(nd1, y1b, __fma_rn(nd2, y2b, __fma_rn(b1, y1a, ya)));
+        const double yc = __fma_rn(nd1, y1c, __fma_rn(nd2, y2c, __fma_rn(b2, y1b, yb)));
+        const double yd = __fma_rn(nd1, y1d, __fma_rn(nd2, y2d, __fma_rn(b3, y1c, yc)));
+        xp = x;
+        y2a = y1a;
+        y1a = ya;
+        y2b = y1b;
+        y1b = yb;
+        y2c = y1c;
+        y1c = yc;
+        y2d = y1d;
+        y1d = yd;
+        acc = __fma_rn(yd, yd, acc);
+    }
+};
+
 template <bool kDirectI>
 __device__ inline void filter_tile(const double (*__restrict__ wx)[kRowPad], int q, int count,
                                    const FastBandCoeffs &k, F64Pair &A, F64Pair &B, F32Stage (&st)[2],
@@ -146,10 +172,31 @@ __device__ inline void filter_tile(const double (*__restrict__ wx)[kRowPad], int
     }
 }
 
-// One tile (16 frames x all bands of one job) of the FP32 form. raw, wx:
+// The same tile position filtered by the FP64-FMA form: all four stages in
+// f64, the squares summed in f64 per sample. The windowed samples are the
+// products the unstaged kernel forms (sample x Hann value, zero outside the
+// signal), so both kernels give the same bits.
+__device__ inline void filter_tile64(const double (*__restrict__ wx)[kRowPad], int q, int count,
+                                     const FastBandCoeffs &k, Cascade64 &A, Cascade64 &B) {
+    const double b0 = k.beta64[0], b1 = k.beta64[1], b2 = k.beta64[2], b3 = k.beta64[3];
+    const double nd1 = -k.d1, nd2 = -k.d2;
+    auto step = [&](int i) {
+        const double2 w = *reinterpret_cast<const double2 *>(&wx[i][q]);
+        A.step(w.x, b0, b1, b2, b3, nd1, nd2);
+        B.step(w.y, b0, b1, b2, b3, nd1, nd2);
+    };
+    if (count == kTileS) {
+#pragma unroll 4
+        for (int i = 0; i < kTileS; ++i) step(i);
+    } else {
+        for (int i = 0; i < count; ++i) step(i);
+    }
+}
+
+// One tile (16 frames x all bands of one job) of the FP32 form (kF64: of the FP64-FMA form). raw, wx:
 // the CTA's shared-memory staging (raw[2][16][kTileS] signal samples,
 // frame-major; wx[2][kTileS][kRowPad] windowed samples, sample-major).
-template <int kThreads>
+template <int kThreads, bool kF64>
 __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__restrict__ jobs,
                                           const FastBandCoeffs *__restrict__ coeffs, int nb,
                                           const double *__restrict__ hann, int window, int hop,
@@ -203,6 +250,7 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
     F32Stage st[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) st[s] = F32Stage{f2(0.f), f2(0.f), f2(0.f)};
+    Cascade64 CA, CB;  // kF64
     double acc_a = 0.0, acc_b = 0.0;
     // Tile t+1's copies are in flight while tile t is filtered; its windowing
     // waits for them (and for every thread to be done reading the buffers it
@@ -212,7 +260,9 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
         const bool more = i0 + kTileS < window;
         if (more) fetch(i0 + kTileS, buf ^ 1);
         const int count = window - i0 < kTileS ? window - i0 : kTileS;
-        if (k.direct_i)
+        if constexpr (kF64)
+            filter_tile64(wx[buf], q, count, k, CA, CB);
+        else if (k.direct_i)
             filter_tile<true>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
         else
             filter_tile<false>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
@@ -223,6 +273,10 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
             __syncthreads();
         }
         buf ^= 1;
+    }
+    if constexpr (kF64) {
+        acc_a = CA.acc;
+        acc_b = CB.acc;
     }
     if (band_raw < nb && f < job.nf) {
         const double inv_n = 1.0 / (double)window;
@@ -237,15 +291,17 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
 // few spills). kPersistent: a grid of kCtasPerSm CTAs per SM takes tiles
 // from a device-side work queue (an atomic counter over the tile list, zero
 // at launch) instead of one CTA per tile. Both choices are measured by the
-// autotuner; every tile is computed the same either way.
-template <int kThreads, int kCtasPerSm, bool kPersistent>
+// autotuner; every tile is computed the same either way. kF64: the FP64-FMA
+// form on the same staged tiles (2 CTAs per SM: 128 registers at 256
+// threads).
+template <int kThreads, int kCtasPerSm, bool kPersistent, bool kF64 = false>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammatone_fast_kernel(
     const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, int ntiles, int *__restrict__ queue,
     const FastBandCoeffs *__restrict__ coeffs, int nb, const double *__restrict__ hann, int window, int hop) {
     __shared__ __align__(16) double raw[2][kCtaFrames][kTileS];
     __shared__ __align__(16) double wx[2][kTileS][kRowPad];
     if constexpr (!kPersistent) {
-        fast_tile<kThreads>(tiles[blockIdx.x], jobs, coeffs, nb, hann, window, hop, raw, wx);
+        fast_tile<kThreads, kF64>(tiles[blockIdx.x], jobs, coeffs, nb, hann, window, hop, raw, wx);
     } else {
         __shared__ int next;
         for (;;) {
@@ -253,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammato
             __syncthreads();
             const int ti = next;
             if (ti >= ntiles) return;  // the same for the whole CTA
-            fast_tile<kThreads>(tiles[ti], jobs, coeffs, nb, hann, window, hop, raw, wx);
+            fast_tile<kThreads, kF64>(tiles[ti], jobs, coeffs, nb, hann, window, hop, raw, wx);
             __syncthreads();  // staging buffers and `next` free for the next tile
         }
     }
@@ -274,30 +330,6 @@ struct Checked {
 __device__ inline bool window_inside(const VSig &sig, int64_t k0, int64_t span) {
     return k0 - sig.head >= 0 && k0 + span - sig.head <= sig.avail;
 }
-
-// Two frames per thread (the second hop samples later): two independent
-// recurrences give each warp twice the FP64 work between dependent steps.
-struct Cascade64 {
-    double xp = 0.0, y1a = 0.0, y2a = 0.0, y1b = 0.0, y2b = 0.0, y1c = 0.0, y2c = 0.0, y1d = 0.0, y2d = 0.0;
-    double acc = 0.0;
-    __device__ inline void step(double x, double b0, double b1, double b2, double b3, double nd1, double nd2) {
-        // stage k input v, previous input = stage k-1's previous output
-        const double ya = __fma_rn(nd1, y1a, __fma_rn(nd2, y2a, __fma_rn(b0, xp, x)));
-        const double yb = __fma_rn(nd1, y1b, __fma_rn(nd2, y2b, __fma_rn(b1, y1a, ya)));
-        const double yc = __fma_rn(nd1, y1c, __fma_rn(nd2, y2c, __fma_rn(b2, y1b, yb)));
-        const double yd = __fma_rn(nd1, y1d, __fma_rn(nd2, y2d, __fma_rn(b3, y1c, yc)));
-        xp = x;
-        y2a = y1a;
-        y1a = ya;
-        y2b = y1b;
-        y1b = yb;
-        y2c = y1c;
-        y1c = yc;
-        y2d = y1d;
-        y1d = yd;
-        acc = __fma_rn(yd, yd, acc);
-    }
-};
 
 template <class Load>
 __device__ void cascade64x2(const Load &sample, int64_t ka, int64_t kb, const FastBandCoeffs &kc,
@@ -471,6 +503,30 @@ void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int nti
     const int threads = (frames_per_cta / 2) * nb;
     gammatone_f64fma_kernel<<<ntiles, threads, 0, s>>>(d_jobs, static_cast<const Tile *>(d_tiles), d_coeffs, nb,
                                                       d_hann, window, hop);
+    launch_counter() += 1;
+}
+
+// The staged kernel first: it measured 0.82 of the FP64 FMA pipe's peak in
+// isolation at 32 bands against 0.75 for the unstaged one.
+std::vector<int> gammatone_f64_staged_candidates() { return {1, 0}; }
+
+void launch_gammatone_f64_staged(const SpecJob *d_jobs, const void *d_tiles, int ntiles,
+                                 const FastBandCoeffs *d_coeffs, int nb, const double *d_hann, int window, int hop,
+                                 cudaStream_t s) {
+    if (ntiles <= 0) return;
+    const Tile *t = static_cast<const Tile *>(d_tiles);
+#define VQB_F64S(T) \
+    gammatone_fast_kernel<T, 2, false, true><<<ntiles, T, 0, s>>>(d_jobs, t, ntiles, nullptr, d_coeffs, nb, d_hann, \
+                                                                  window, hop)
+    if (nb > 24)
+        VQB_F64S(256);
+    else if (nb > 16)
+        VQB_F64S(192);
+    else if (nb > 8)
+        VQB_F64S(128);
+    else
+        VQB_F64S(64);
+#undef VQB_F64S
     launch_counter() += 1;
 }
 

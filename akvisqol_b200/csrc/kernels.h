@@ -145,6 +145,14 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
 std::vector<int> gammatone_f64fma_frames_candidates(int nb);
 void launch_gammatone_f64fma(const SpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
                              int nb, const double *d_hann, int window, int hop, int frames_per_cta, cudaStream_t s);
+// The f64 FMA form on the FP32 kernel's staged tiles (tiles of
+// gammatone_fast_frames_per_cta() frames): the same bits as
+// launch_gammatone_f64fma. Candidates of the autotuner: 1 = this one (the
+// default), 0 = that kernel.
+std::vector<int> gammatone_f64_staged_candidates();
+void launch_gammatone_f64_staged(const SpecJob *d_jobs, const void *d_tiles, int ntiles,
+                                 const FastBandCoeffs *d_coeffs, int nb, const double *d_hann, int window, int hop,
+                                 cudaStream_t s);
 
 // k_spec.cu
 // Spectrogram preparation of njobs pairs (max_frames = the largest nfr or

@@ -657,6 +657,6 @@ def autotune_choices() -> list[dict]:
     rows = (c_int32 * (5 * max(1, n.value)))()
     _check(lib.visqol_b200_autotune_choices(rows, n.value, ctypes.byref(n)))
     names = {0: "gammatone_frames_per_cta", 1: "nsim_table_offsets_per_cta", 2: "lag_column_passes",
-             3: "gammatone_fast_shape"}
+             3: "gammatone_fast_shape", 4: "gammatone_f64_staged"}
     return [{"device": rows[5 * i], "kernel": names.get(rows[5 * i + 1], str(rows[5 * i + 1])),
              "variant": (rows[5 * i + 2], rows[5 * i + 3]), "choice": rows[5 * i + 4]} for i in range(n.value)]

@@ -167,8 +167,9 @@ int visqol_b200_lattice_predict(const char *model_path, size_t nb, const double 
  * {device, kernel (0 gammatone frames per CTA, 1 NSIM-table offsets per
  * CTA, 2 lag-search column passes: 0 shared-memory tiles, 1 registers, 3
  * FP32-form gammatone: CTAs per SM (its register budget), + 100 for the
- * persistent form that takes its tiles from a device-side work queue),
- * variant a (form / cell arithmetic / log2 transform size), variant b
+ * persistent form that takes its tiles from a device-side work queue, 4
+ * FP64-FMA-form gammatone: 0 its own kernel, 1 on the FP32 kernel's staged
+ * tiles), variant a (form / cell arithmetic / log2 transform size), variant b
  * (bands / raw signals), choice},
  * written to rows up to max_rows. Each kernel class is measured on its
  * first batch per device (candidate shapes write identical results);

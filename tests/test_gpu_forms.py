@@ -99,3 +99,32 @@ def test_fast_gammatone_shapes_agree(native, monkeypatch, shape):
         assert c0 == c1 == 0
         assert r0["moslqo"] == r1["moslqo"]
         assert np.array_equal(r0["fvnsim"], r1["fvnsim"])
+
+
+@pytest.mark.parametrize("mode", ["audio", "speech"])
+def test_balanced_gammatone_kernels_agree(native, monkeypatch, mode):
+    """The FP64-FMA form's two gammatone kernels (its own, which forms each
+    windowed sample in a lane and shuffles it to the warp; and the FP32
+    kernel's staged shared-memory tiles with all four stages in f64) filter
+    the same windowed samples with the same FMA order: identical bits for
+    32 bands (audio) and 21 (speech)."""
+    from akvisqol_b200 import synth
+    if mode == "audio":
+        pairs = synth.audio_batch(4, seed0=synth.SEED_BASE + 720, min_s=2.0, max_s=6.0)
+        sr, ctx = 48000, native.Context(mode=native.MODE_AUDIO, precision="balanced")
+    else:
+        pairs = synth.speech_batch(4, seed0=synth.SEED_BASE + 740, min_s=2.0, max_s=6.0)
+        sr = 16000
+        ctx = native.Context(mode=native.MODE_SPEECH, use_lattice_model=False, precision="balanced")
+    refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
+    monkeypatch.setenv("VISQOL_TUNE_4", "0")
+    base = ctx.measure_batch_traced(refs, degs, sr)
+    monkeypatch.setenv("VISQOL_TUNE_4", "1")
+    got = ctx.measure_batch_traced(refs, degs, sr)
+    for (c0, r0, t0), (c1, r1, t1) in zip(base, got):
+        assert c0 == c1 == 0
+        assert r0["moslqo"] == r1["moslqo"]
+        for key in ("fvnsim", "fvnsim10", "fstdnsim", "fvdegenergy"):
+            assert np.array_equal(r0[key], r1[key]), key
+        for key in DISCRETE:
+            assert np.array_equal(t0[key], t1[key]), key
