@@ -7,8 +7,12 @@
 // the band gain become one f64 factor on the RMS), so a stage is three FMAs:
 // y = v + beta v[-1] - d2 y[-2] - d1 y[-1]. 13 FMAs and one multiply per
 // sample instead of the exact form's 31 separately rounded operations; the
-// results stay within ~1e-13 of the exact form in MOS. Thread and warp
-// layout as the exact kernel (a warp reads one sample per step, broadcast).
+// results stay within ~1e-13 of the exact form in MOS. Two kernels compute
+// it with the same bits: by default the f32 form's kernel below with all
+// four stages in f64 (its staged shared-memory tiles, one 16-byte load per
+// step for a thread's two frames), and gammatone_f64fma_kernel, whose
+// thread and warp layout is the exact kernel's (a lane forms one windowed
+// sample and the warp reads it by shuffle); the autotuner measures both.
 //
 // f32 form (gammatone_fast_kernel) splits the cascade across the two
 // arithmetic pipes of an SM:
