@@ -101,17 +101,22 @@ def test_fast_gammatone_shapes_agree(native, monkeypatch, shape):
         assert np.array_equal(r0["fvnsim"], r1["fvnsim"])
 
 
-@pytest.mark.parametrize("mode", ["audio", "speech"])
+@pytest.mark.parametrize("mode", ["audio", "audio44k", "speech"])
 def test_balanced_gammatone_kernels_agree(native, monkeypatch, mode):
     """The FP64-FMA form's two gammatone kernels (its own, which forms each
     windowed sample in a lane and shuffles it to the warp; and the FP32
     kernel's staged shared-memory tiles with all four stages in f64) filter
     the same windowed samples with the same FMA order: identical bits for
-    32 bands (audio) and 21 (speech)."""
+    32 bands (audio) and 21 (speech), and at 44.1 kHz, whose 3528-sample
+    window ends on a partial tile."""
     from akvisqol_b200 import synth
     if mode == "audio":
         pairs = synth.audio_batch(4, seed0=synth.SEED_BASE + 720, min_s=2.0, max_s=6.0)
         sr, ctx = 48000, native.Context(mode=native.MODE_AUDIO, precision="balanced")
+    elif mode == "audio44k":
+        sr = 44100
+        pairs = [synth.audio_pair(synth.SEED_BASE + 730 + i, seconds=3.0, sample_rate=sr) for i in range(3)]
+        ctx = native.Context(mode=native.MODE_AUDIO, precision="balanced")
     else:
         pairs = synth.speech_batch(4, seed0=synth.SEED_BASE + 740, min_s=2.0, max_s=6.0)
         sr = 16000
@@ -128,3 +133,45 @@ def test_balanced_gammatone_kernels_agree(native, monkeypatch, mode):
             assert np.array_equal(r0[key], r1[key]), key
         for key in DISCRETE:
             assert np.array_equal(t0[key], t1[key]), key
+
+
+_RATE_CASES = {}
+
+
+def _rate_case(oracle, sr):
+    """Two 4 s audio pairs at sample rate sr and the oracle's results
+    (computed once per rate for all forms). The second pair's degraded
+    signal gains 7 samples of delay half way through, so the first half's
+    patches realign by 7 samples: off the frame grid, their slice
+    spectrograms are recomputed instead of copied."""
+    if sr not in _RATE_CASES:
+        from akvisqol_b200 import synth
+        pairs = [synth.audio_pair(synth.SEED_BASE + 900 + i, seconds=4.0, sample_rate=sr,
+                                  cutoff_hz=0.4 * sr) for i in range(2)]
+        ref, deg = pairs[1]
+        k = len(deg) // 2
+        pairs[1] = (ref, np.concatenate([deg[:k], np.zeros(7), deg[k:]]))
+        _RATE_CASES[sr] = (pairs, [oracle.measure(r, d, sr) for r, d in pairs])
+    return _RATE_CASES[sr]
+
+
+@pytest.mark.parametrize("sr", [44100, 22050])
+@pytest.mark.parametrize("form,tol", [("exact", 1e-12), ("balanced", 1e-10), ("fast", 1e-5)])
+def test_other_sample_rates(native, oracle, sr, form, tol):
+    """Audio mode at 44.1 and 22.05 kHz: windows of 3528 and 1764 samples,
+    not multiples of the staged gammatone kernels' 64-sample tiles, so each
+    frame ends on a partial tile; transform sizes and frame geometry other
+    than the 48 kHz ones. Every form against the oracle, decisions
+    identical."""
+    pairs, wants = _rate_case(oracle, sr)
+    assert any(lag != 0 for lag in wants[1][1]["realign_lag"])
+    ctx = native.Context(mode=native.MODE_AUDIO, precision=form)
+    got = run(ctx, pairs, sr)
+    for (code, res, tr), (want, wtr) in zip(got, wants):
+        assert code == 0
+        assert abs(res["moslqo"] - want["moslqo"]) <= tol, (res["moslqo"], want["moslqo"])
+        assert tr["global_lag"] == wtr["global_lag"]
+        for key in ("deg_len", "nf_ref", "nf_deg", "num_patches"):
+            assert tr[key] == wtr[key], key
+        for key in DISCRETE:
+            assert np.array_equal(tr[key], wtr[key]), key
