@@ -291,8 +291,8 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
 }
 
 // kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21. kCtasPerSm
-// sets the register budget (3: 80 registers at 256 threads; 4: 64, with a
-// few spills). kPersistent: a grid of kCtasPerSm CTAs per SM takes tiles
+// sets the register budget (2: 108 registers at 256 threads, no spills; 3:
+// 80, a few spills; 4: 64, more). kPersistent: a grid of kCtasPerSm CTAs per SM takes tiles
 // from a device-side work queue (an atomic counter over the tile list, zero
 // at launch) instead of one CTA per tile. Both choices are measured by the
 // autotuner; every tile is computed the same either way. kF64: the FP64-FMA
@@ -440,12 +440,12 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
 }
 
 // Launch shapes: CTAs per SM (register budget) + 100 for the persistent
-// work-queue form. The autotuner measures the first two; the persistent
+// work-queue form. The autotuner measures the first three; the persistent
 // shapes measured ~4.5% slower inside the four-lane batch pipeline (their
 // resident CTAs hold SMs the other lanes' kernels would take) and are
 // selected only by VISQOL_TUNE_3.
-std::vector<int> gammatone_fast_shape_candidates() { return {3, 4}; }
-std::vector<int> gammatone_fast_shapes() { return {3, 4, 103, 104}; }
+std::vector<int> gammatone_fast_shape_candidates() { return {3, 4, 2}; }
+std::vector<int> gammatone_fast_shapes() { return {3, 4, 2, 103, 104}; }
 
 namespace {
 int sm_count() {
@@ -475,6 +475,8 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
             VQB_FAST(T, 3, true);        \
     } else if (ctas == 4) {              \
         VQB_FAST(T, 4, false);           \
+    } else if (ctas == 2) {              \
+        VQB_FAST(T, 2, false);           \
     } else {                             \
         VQB_FAST(T, 3, false);           \
     }
