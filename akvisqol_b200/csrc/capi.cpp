@@ -179,6 +179,17 @@ bool first_of_its_kind(const visqol_ctx *c, uint32_t sample_rate) {
     return seen.insert(key).second;
 }
 
+// Joins the threads it holds when it goes out of scope, so that an exception
+// while starting them (a thread that cannot be created) never destroys a
+// joinable std::thread; the threads' work ends by itself.
+struct JoinAll {
+    std::vector<std::thread> threads;
+    ~JoinAll() {
+        for (auto &t : threads)
+            if (t.joinable()) t.join();
+    }
+};
+
 // Host-input batches through all lanes at once: the signals go up in chunks
 // of consecutive pairs, in order, on a copy stream of their own (one copy in
 // flight, so the lanes' own small uploads never queue behind a whole chunk),
@@ -249,7 +260,8 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
     size_t recorded = 0;
     bool failed = false;
     std::exception_ptr upload_error;
-    std::thread uploader([&] {
+    JoinAll uploader;
+    uploader.threads.emplace_back([&] {
         try {
             VQB_CUDA(cudaSetDevice(device));
             size_t copies = 0;
@@ -322,17 +334,17 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
         for (size_t k = next++; k < nk; k = next++)
             if (!score_chunk(l, k)) return;
     };
-    std::vector<std::thread> threads;
+    JoinAll lanes;
     if (alone_first) {
         // lane 0 scores chunk 0 alone (the autotuner measures there), then
         // all lanes share the remaining chunks
         next = 1;
         score_chunk(0, 0);
     }
-    for (size_t l = 1; l < L; ++l) threads.emplace_back(work, l);
+    for (size_t l = 1; l < L; ++l) lanes.threads.emplace_back(work, l);
     work(0);
-    for (auto &t : threads) t.join();
-    uploader.join();
+    for (auto &t : lanes.threads) t.join();
+    uploader.threads[0].join();
     if (upload_error) std::rethrow_exception(upload_error);
     for (auto &e : errs)
         if (e) std::rethrow_exception(e);
@@ -413,13 +425,13 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
             errs[l] = std::current_exception();
         }
     };
-    std::vector<std::thread> threads;
+    JoinAll lanes;
     // the first batch of its kind: lane 0's share alone (the autotuner
     // measures there), then the other lanes
     if (alone_first) work(0);
-    for (size_t l = 1; l < L; ++l) threads.emplace_back(work, l);
+    for (size_t l = 1; l < L; ++l) lanes.threads.emplace_back(work, l);
     if (!alone_first) work(0);
-    for (auto &t : threads) t.join();
+    for (auto &t : lanes.threads) t.join();
     for (auto &e : errs)
         if (e) std::rethrow_exception(e);
     vqb::Timing t{};

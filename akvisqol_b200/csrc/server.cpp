@@ -95,6 +95,20 @@ struct visqol_b200_server {
     };
     std::vector<std::unique_ptr<Lane>> lanes;
 
+    // Stops the lanes (each finishes its batch in flight and what is still
+    // queued) and joins them: visqol_b200_server_destroy, and the cleanup
+    // when creation fails after some lanes started.
+    ~visqol_b200_server() {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            stopping = true;
+        }
+        cv_work.notify_all();
+        for (auto &l : lanes)
+            if (l->thread.joinable()) l->thread.join();
+        for (auto &d : done) visqol_result_free(d.result);
+    }
+
     vqb::Engine &engine(Lane &l, uint32_t mode) {
         auto &e = l.engine[mode];
         if (!e) e = std::make_unique<vqb::Engine>(device, opt[mode], mode == 0 ? svr : nullptr,
@@ -170,7 +184,13 @@ struct visqol_b200_server {
             visqol_result *res = nullptr;
             if (code == VISQOL_OK) {
                 code = out[i].code;
-                if (code == VISQOL_OK) res = vqb::box_result(std::move(out[i].scores));
+                if (code == VISQOL_OK) {
+                    try {
+                        res = vqb::box_result(std::move(out[i].scores));
+                    } catch (const std::bad_alloc &) {
+                        code = VISQOL_E_OUT_OF_MEMORY;
+                    }
+                }
             }
             finished[i] = Done{batch[i]->ticket, code, res};
         }
@@ -256,18 +276,7 @@ int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serv
     return VISQOL_OK;
 }
 
-void visqol_b200_server_destroy(visqol_b200_server *s) {
-    if (!s) return;
-    {
-        std::lock_guard<std::mutex> lock(s->mu);
-        s->stopping = true;
-    }
-    s->cv_work.notify_all();
-    for (auto &l : s->lanes)
-        if (l->thread.joinable()) l->thread.join();
-    for (auto &d : s->done) visqol_result_free(d.result);
-    delete s;
-}
+void visqol_b200_server_destroy(visqol_b200_server *s) { delete s; }
 
 int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double *ref, size_t ref_len,
                               const double *deg, size_t deg_len, uint32_t sample_rate, uint32_t flags,

@@ -153,7 +153,9 @@ int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double
 int visqol_b200_server_next(visqol_b200_server *s, int32_t timeout_ms, uint64_t *ticket, int32_t *status,
                             visqol_result **out);
 /* Counters and latency percentiles; reset != 0 clears the latency samples
- * and the batch counters after reading. */
+ * and the batch counters after reading. The server keeps two doubles per
+ * completed request (latency, queueing) until a reset, so a long-running
+ * caller resets periodically. */
 int visqol_b200_server_stats(visqol_b200_server *s, visqol_b200_serve_stats *out, int reset);
 
 /* The speech-mode TF-Lattice MOS mapping alone, on the host (reference
