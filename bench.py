@@ -18,7 +18,9 @@ are timed the same way and reported under "forms", each with its largest
   python bench.py --impl reference ...   # the reference CPU model (oracle), all host threads
 
 With torchrun (N > 1) every rank scores its own batch (weak scaling, no
-collective on the data path); the step time is the maximum over ranks.
+collective on the data path); the step time is the maximum over ranks. The
+uneven batches and the serving sweep are one-GPU measurements and run at
+N = 1 only.
 """
 
 from __future__ import annotations
@@ -556,9 +558,11 @@ def run_ours(args, rank, world, local):
         "prepared_references": prepared_line,
         "autotune": native.autotune_choices(),
     }
-    if args.config_pairs > 0 and rank == 0:
+    # The uneven batches and the serving sweep are one-GPU measurements: a
+    # multi-rank run (weak scaling of the batch step) leaves them to N = 1.
+    if args.config_pairs > 0 and rank == 0 and world == 1:
         line["uneven_batches"] = uneven_configs(native, torch, args.config_pairs, plain_value)
-    if args.serve_requests > 0:
+    if args.serve_requests > 0 and world == 1:
         pool = serve_pool(0x5EED_4000 + 7919 * rank)
         line["serving"] = {f: serve_sweep(native, torch, f, pool, args.serve_requests, 17 + rank)
                            for f in dict.fromkeys([args.precision, "balanced", "exact"])}
