@@ -853,6 +853,9 @@ int visqol_b200_last_timing(visqol_ctx *c, visqol_b200_timing *out) {
     out->h2d_bytes = t.h2d_bytes;
     out->d2h_bytes = t.d2h_bytes;
     out->host_syncs = t.host_syncs;
+    out->lag_kernel_ms = t.lag_kernel_ms;
+    out->lag_bytes = t.lag_bytes;
+    out->lag_reruns = t.lag_reruns;
     return VISQOL_OK;
 }
 

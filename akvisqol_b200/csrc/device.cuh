@@ -41,6 +41,20 @@ struct SpecJob {
     double *out;
 };
 
+// Lag candidates the f32 correlation nominates (reference
+// src/xcorr.zig:270-340): at most this many are rescored in f64.
+constexpr int kLagCandCap = 64;
+
+// One CTA's nomination record in the f32 lag search: its largest |Re| over
+// valid lags, and every lag within the slack of that maximum (count may
+// exceed kLagCandCap; then only the first kLagCandCap are stored).
+struct LagCands {
+    float top;
+    int32_t count;
+    float v[kLagCandCap];
+    int32_t key[kLagCandCap];
+};
+
 // One lag search: FFT cross-correlation of the upper envelopes of a and b
 // (reference src/accel.zig:100-107), or of a and b themselves (raw).
 struct LagJob {
@@ -51,6 +65,16 @@ struct LagJob {
     double *stats_a, *stats_b;
     double2 *z;          // n complex values
     int64_t *lag_out;
+    // f32 search (FP32 form): f32 transform, f64 rescoring of the near-maxima
+    float2 *z32;         // n complex values
+    double2 *energy;     // per forward CTA: sums of squares of a's and b's envelopes
+    LagCands *cands;     // per inverse CTA
+    int32_t *status;     // 0: lag decided; 1: over kLagCandCap candidates, the f64 search decides
+    int32_t *ncand;      // candidates above the job's floor
+    int32_t *cand_key;   // kLagCandCap of them
+    double *rescore;     // kLagCandCap x chunks partial dot products
+    float *corr_out;     // test only (else null): Re of the f32 correlation, n values
+    double slack_fixed;  // test only (else 0): the nomination slack, instead of the f32 error bound
 };
 
 // Serial reductions over a signal, in the CPU's order, into

@@ -94,6 +94,11 @@ void *Arena::alloc(size_t bytes) {
     current_ = chunks_.size() - 1;
     return c.base;
 }
+void Arena::release() {
+    for (auto &c : chunks_) cudaFree(c.base);
+    chunks_.clear();
+    current_ = 0;
+}
 size_t Arena::reserved() const {
     size_t s = 0;
     for (auto &c : chunks_) s += c.size;
@@ -151,8 +156,10 @@ Engine::Engine(int device, const Options &opt, std::shared_ptr<const host::Svr> 
     events_.resize(8);
     for (auto &e : events_) VQB_CUDA(cudaEventCreate(&e));
     for (auto &e : gt_events_) VQB_CUDA(cudaEventCreate(&e));
+    for (auto &e : lag_events_) VQB_CUDA(cudaEventCreate(&e));
     fft_init_attributes();
     lag_init_attributes();
+    lag32_init_attributes();
     nsim_init_attributes();
     VQB_CUDA(cudaGetLastError());
 }
@@ -179,7 +186,22 @@ Engine::~Engine() {
     for (auto e : events_) cudaEventDestroy(e);
     for (auto e : gt_events_)
         if (e) cudaEventDestroy(e);
+    for (auto e : lag_events_)
+        if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::release_device_memory() {
+    VQB_CUDA(cudaSetDevice(device_));
+    VQB_CUDA(cudaStreamSynchronize(stream_));
+    VQB_CUDA(cudaStreamSynchronize(side_));
+    VQB_CUDA(cudaStreamSynchronize(copy_));
+    arena_.release();
+    for (int k = 0; k < 2; ++k) {
+        if (slot_[k]) cudaFree(slot_[k]);
+        slot_[k] = nullptr;
+        slot_bytes_[k] = 0;
+    }
 }
 
 const Engine::RateCache &Engine::rate_cache(uint32_t sr) {
@@ -223,13 +245,20 @@ Engine::Twiddles Engine::twiddles(size_t n) {
         t.resize(stages_at + block_stage_twiddle_count());
         fill_block_stage_twiddles(t.data() + half, t.data() + stages_at);
     }
+    // f32 copies of the block, column and stage tables (the f32 search)
+    std::vector<float2> t32(t.size() - half);
+    for (size_t k = half; k < t.size(); ++k) t32[k - half] = make_float2((float)t[k].x, (float)t[k].y);
+    // one allocation: the f64 tables, then the f32 ones at a 16-byte boundary
+    const size_t bytes64 = std::max<size_t>(1, t.size()) * sizeof(double2);
     double2 *d = nullptr;
-    VQB_CUDA(cudaMalloc(&d, std::max<size_t>(1, t.size()) * sizeof(double2)));
+    VQB_CUDA(cudaMalloc(&d, bytes64 + std::max<size_t>(1, t32.size()) * sizeof(float2)));
+    float2 *d32 = reinterpret_cast<float2 *>(reinterpret_cast<char *>(d) + bytes64);
     if (!t.empty()) {
         VQB_CUDA(cudaMemcpyAsync(d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, stream_));
+        VQB_CUDA(cudaMemcpyAsync(d32, t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice, stream_));
         VQB_CUDA(cudaStreamSynchronize(stream_));
     }
-    Twiddles tw{d, d + half, d + cols_at, d + stages_at};
+    Twiddles tw{d, d + half, d + cols_at, d + stages_at, d32, d32 + (cols_at - half), d32 + (stages_at - half)};
     twiddles_[n] = tw;
     return tw;
 }
@@ -268,18 +297,61 @@ float Engine::elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
-    if (jobs.empty()) return;
+uint64_t lag_search_bytes(const LagJob &j, bool f32) {
+    // signals read by the forward pass (and by the f32 search's rescoring),
+    // then the transform written, read and written, read: 4 passes over z
+    const uint64_t sig = 8 * (uint64_t)(j.a.avail + j.b.avail);
+    return f32 ? 2 * sig + 4 * 8 * (uint64_t)j.n : sig + 4 * 16 * (uint64_t)j.n;
+}
+
+int32_t *Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw, bool exact) {
+    if (jobs.empty()) return nullptr;
     // Group by FFT size; bound each submission's buffer.
     std::map<int64_t, std::vector<size_t>> groups;
     for (size_t i = 0; i < jobs.size(); ++i) groups[jobs[i].n].push_back(i);
     const size_t budget = size_t(4) << 30;
+    const bool f32 = opt_.form == kFormF32 && !exact;
+    int32_t *d_status = nullptr;
+    if (f32) {
+        d_status = arena_.alloc_n<int32_t>(jobs.size());
+        launch_zero(d_status, jobs.size() * sizeof(int32_t), stream_);
+    }
     for (auto &g : groups) {
         const int64_t n = g.first;
         const Twiddles tw = twiddles((size_t)n);
         const size_t per = std::max<size_t>(1, budget / ((size_t)n * sizeof(double2)));
         for (size_t c0 = 0; c0 < g.second.size(); c0 += per) {
             const size_t cnt = std::min(per, g.second.size() - c0);
+            if (f32 && fused_lag_supported(n)) {
+                // The f32 search (half the transform's bytes, FP32 arithmetic),
+                // then f64 rescoring of its candidates.
+                const size_t parts = lag32_parts(n);
+                int64_t max_b = 1;
+                for (size_t k = 0; k < cnt; ++k) max_b = std::max(max_b, jobs[g.second[c0 + k]].b.len);
+                const int nchunks = lag32_rescore_chunks(max_b);
+                float2 *z = arena_.alloc_n<float2>((size_t)n * cnt);
+                double2 *energy = arena_.alloc_n<double2>(parts * cnt);
+                LagCands *cands = arena_.alloc_n<LagCands>(parts * cnt);
+                int32_t *ncand = arena_.alloc_n<int32_t>(cnt);
+                int32_t *keys = arena_.alloc_n<int32_t>((size_t)kLagCandCap * cnt);
+                double *rescore = arena_.alloc_n<double>((size_t)kLagCandCap * nchunks * cnt);
+                std::vector<LagJob> chunk(cnt);
+                for (size_t k = 0; k < cnt; ++k) {
+                    const size_t i = g.second[c0 + k];
+                    LagJob j = jobs[i];
+                    j.z32 = z + (int64_t)k * n;
+                    j.energy = energy + k * parts;
+                    j.cands = cands + k * parts;
+                    j.status = d_status + i;
+                    j.ncand = ncand + k;
+                    j.cand_key = keys + (size_t)kLagCandCap * k;
+                    j.rescore = rescore + (size_t)kLagCandCap * nchunks * k;
+                    chunk[k] = j;
+                }
+                launch_lag32(upload(chunk), (int)cnt, n, raw, tw.cols32, tw.block32, tw.stages32, nchunks, stream_);
+                continue;
+            }
+            // (above 2^24 points the exact search decides in every form; status stays 0)
             double2 *z = arena_.alloc_n<double2>((size_t)n * cnt);
             std::vector<LagJob> chunk(cnt);
             for (size_t k = 0; k < cnt; ++k) {
@@ -317,6 +389,18 @@ void Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw) {
             launch_argmax(z, d_jobs, (int)cnt, n, n, pv, pk, stream_);
         }
     }
+    return d_status;
+}
+
+std::vector<size_t> Engine::rerun_undecided(const std::vector<LagJob> &jobs, const int32_t *h_status, bool raw) {
+    std::vector<size_t> idx;
+    if (!h_status) return idx;
+    std::vector<LagJob> rerun;
+    for (size_t i = 0; i < jobs.size(); ++i)
+        if (h_status[i]) idx.push_back(i), rerun.push_back(jobs[i]);
+    if (!rerun.empty()) launch_lag_jobs(rerun, raw, true);
+    timing_.lag_reruns += idx.size();
+    return idx;
 }
 
 size_t Engine::pair_footprint(size_t rl, size_t dl, uint32_t sample_rate, bool speech) {
@@ -581,7 +665,8 @@ void Engine::launch_sums(const std::vector<SumJob> &sums) {
         launch_envelope_stats(d, (int)sums.size(), stream_);
 }
 
-void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags) {
+void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags, int32_t *status_out,
+                  float *d_corr) {
     arena_.reset();
     pinned_.reset();
     std::vector<LagJob> jobs(njobs);
@@ -597,6 +682,7 @@ void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t 
         j.stats_a = d_stats + 8 * i;
         j.stats_b = d_stats + 8 * i + 4;
         j.lag_out = d_lags + i;
+        j.corr_out = i == 0 ? d_corr : nullptr;
         sums.push_back(SumJob{a[i], j.stats_a});
         sums.push_back(SumJob{b[i], j.stats_b});
     }
@@ -607,11 +693,49 @@ void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t 
     for (size_t i = 0; i < njobs; ++i)
         if (jobs[i].biggest > 0) run.push_back(jobs[i]), where.push_back(i);
     if (!raw && !sums.empty()) launch_envelope_stats(upload(sums), (int)sums.size(), stream_);
-    launch_lag_jobs(run, raw);
+    int32_t *d_status = launch_lag_jobs(run, raw);
     int64_t *h = pinned_.alloc_n<int64_t>(njobs);
+    int32_t *h_status = d_status ? pinned_.alloc_n<int32_t>(run.size()) : nullptr;
     d2h(h, d_lags, njobs * sizeof(int64_t));
+    if (h_status && !run.empty()) d2h(h_status, d_status, run.size() * sizeof(int32_t));
     sync();
+    if (!rerun_undecided(run, h_status, raw).empty()) {
+        d2h(h, d_lags, njobs * sizeof(int64_t));
+        sync();
+    }
     std::memcpy(h_lags, h, njobs * sizeof(int64_t));
+    if (status_out)
+        for (size_t k = 0; k < run.size(); ++k) status_out[where[k]] = h_status ? h_status[k] : 0;
+}
+
+bool Engine::refine_approx(const VSig &a, const VSig &b, const float *d_approx, int64_t n, double slack,
+                           int64_t *lag) {
+    arena_.reset();
+    pinned_.reset();
+    LagJob j{};
+    j.a = a;
+    j.b = b;
+    j.n = n;
+    j.biggest = std::max(a.len, b.len);
+    const int nchunks = lag32_rescore_chunks(std::max<int64_t>(1, b.len));
+    const size_t parts = (size_t)((n + 4095) / 4096);
+    j.corr_out = const_cast<float *>(d_approx);
+    j.slack_fixed = slack;
+    j.cands = arena_.alloc_n<LagCands>(parts);
+    j.status = arena_.alloc_n<int32_t>(1);
+    j.ncand = arena_.alloc_n<int32_t>(1);
+    j.cand_key = arena_.alloc_n<int32_t>(kLagCandCap);
+    j.rescore = arena_.alloc_n<double>((size_t)kLagCandCap * nchunks);
+    j.lag_out = arena_.alloc_n<int64_t>(1);
+    launch_zero(j.lag_out, sizeof(int64_t), stream_);
+    launch_refine_approx(upload(std::vector<LagJob>{j}), n, nchunks, stream_);
+    int64_t *h = pinned_.alloc_n<int64_t>(1);
+    int32_t *st = pinned_.alloc_n<int32_t>(1);
+    d2h(h, j.lag_out, sizeof(int64_t));
+    d2h(st, j.status, sizeof(int32_t));
+    sync();
+    *lag = *h;
+    return *st == 0;
 }
 
 void Engine::spectrogram(const host::Filterbank &fb, const double *d_hann, size_t window, size_t hop,
@@ -781,9 +905,30 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     // ---- 1: global lag and SPL energies --------------------------------
     int64_t *d_lags = arena_.alloc_n<int64_t>(n);
     launch_zero(d_lags, n * sizeof(int64_t), stream_);
+    std::vector<LagJob> lag_jobs;
+    std::vector<size_t> lag_pair;  // pair of each lag job
+    int32_t *d_lstat = nullptr;    // FP32 form: per lag job, 1 when the f32 search left it undecided
+    // aligned energies (read the lags on the device) of the listed pairs
+    auto launch_aligned = [&](const std::vector<size_t> &pairs) {
+        std::vector<char> args;
+        const size_t asz = aligned_energy_args_size();
+        int na = 0;
+        for (size_t i : pairs) {
+            PairState &s = ps[i];
+            if (!s.live) continue;
+            args.resize(args.size() + asz);
+            fill_aligned_energy_args(args.data() + args.size() - asz, VSig{s.deg, 0, (int64_t)s.dl, (int64_t)s.dl},
+                                     (int64_t)s.rl, d_lags + i, s.stats + 8, s.lag_job ? s.stats + 4 : nullptr);
+            ++na;
+        }
+        if (na && opt_.form != kFormExact)
+            launch_aligned_energy_tree(upload_bytes(args.data(), args.size()), na,
+                                       arena_.alloc_n<double>((size_t)na * kTreeParts * 3), stream_);
+        else if (na)
+            launch_aligned_energy(upload_bytes(args.data(), args.size()), na, stream_);
+    };
     {
         std::vector<SumJob> sums;
-        std::vector<LagJob> lag_jobs;
         for (size_t i = 0; i < n; ++i) {
             PairState &s = ps[i];
             if (!s.live) continue;
@@ -801,35 +946,43 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                 j.stats_b = s.stats + 4;
                 j.lag_out = d_lags + i;
                 lag_jobs.push_back(j);
+                lag_pair.push_back(i);
                 s.trace.fft_nlogn += 2.0 * (double)j.n * std::log2((double)j.n);
+                timing_.lag_bytes += lag_search_bytes(j, opt_.form == kFormF32);
             }
         }
         launch_sums(sums);
-        launch_lag_jobs(lag_jobs, false);
-        std::vector<char> args;
-        const size_t asz = aligned_energy_args_size();
-        int na = 0;
-        for (size_t i = 0; i < n; ++i) {
-            PairState &s = ps[i];
-            if (!s.live) continue;
-            args.resize(args.size() + asz);
-            fill_aligned_energy_args(args.data() + args.size() - asz, VSig{s.deg, 0, (int64_t)s.dl, (int64_t)s.dl},
-                                     (int64_t)s.rl, d_lags + i, s.stats + 8);
-            ++na;
-        }
-        if (na && opt_.form != kFormExact)
-            launch_aligned_energy_tree(upload_bytes(args.data(), args.size()), na,
-                                       arena_.alloc_n<double>((size_t)na * kTreeParts * 3), stream_);
-        else if (na)
-            launch_aligned_energy(upload_bytes(args.data(), args.size()), na, stream_);
+        record(lag_events_[0]);
+        d_lstat = launch_lag_jobs(lag_jobs, false);
+        record(lag_events_[1]);
+        std::vector<size_t> all(n);
+        for (size_t i = 0; i < n; ++i) all[i] = i;
+        launch_aligned(all);
     }
     int64_t *h_lags = pinned_.alloc_n<int64_t>(n);
     double *h_stats = pinned_.alloc_n<double>(10 * n);
+    int32_t *h_lstat = d_lstat ? pinned_.alloc_n<int32_t>(lag_jobs.size()) : nullptr;
     d2h(h_lags, d_lags, n * sizeof(int64_t));
     for (size_t i = 0; i < n; ++i)
         if (ps[i].live) d2h(h_stats + 10 * i, ps[i].stats, 10 * sizeof(double));
+    if (h_lstat) d2h(h_lstat, d_lstat, lag_jobs.size() * sizeof(int32_t));
     record(events_[1]);
     sync();
+    {
+        // searches the f32 pass left undecided: the exact search, then those
+        // pairs' aligned energies again
+        const std::vector<size_t> redo = rerun_undecided(lag_jobs, h_lstat, false);
+        if (!redo.empty()) {
+            std::vector<size_t> pairs;
+            for (size_t k : redo) pairs.push_back(lag_pair[k]);
+            launch_aligned(pairs);
+            for (size_t i : pairs) {
+                d2h(h_lags + i, d_lags + i, sizeof(int64_t));
+                d2h(h_stats + 10 * i, ps[i].stats, 10 * sizeof(double));
+            }
+            sync();
+        }
+    }
     for (size_t i = 0; i < n; ++i)
         if (ps[i].live && ps[i].prep) std::copy(ps[i].prep->stats, ps[i].prep->stats + 4, h_stats + 10 * i);
 
@@ -1064,10 +1217,16 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
         }
         // ---- 5: slice lags --------------------------------------------------
         launch_sums(slice_sums);
-        launch_lag_jobs(slice_lags, false);
+        int32_t *d_sstat = launch_lag_jobs(slice_lags, false);
         int64_t *h_sl = pinned_.alloc_n<int64_t>(n_slices);
+        int32_t *h_sstat = d_sstat ? pinned_.alloc_n<int32_t>(n_slices) : nullptr;
         d2h(h_sl, d_slice_lags, n_slices * sizeof(int64_t));
+        if (h_sstat) d2h(h_sstat, d_sstat, n_slices * sizeof(int32_t));
         sync();
+        if (!rerun_undecided(slice_lags, h_sstat, false).empty()) {
+            d2h(h_sl, d_slice_lags, n_slices * sizeof(int64_t));
+            sync();
+        }
 
         // ---- 6: trimmed geometry, frame reuse (host) -------------------------
         std::vector<SpecJob> rjobs;
@@ -1165,6 +1324,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     VQB_CUDA(cudaEventSynchronize(events_[7]));
     for (uint64_t g = 0; g < timing_.gammatone_launches; ++g)
         timing_.gammatone_kernel_ms += elapsed(gt_events_[2 * g], gt_events_[2 * g + 1]);
+    if (!lag_jobs.empty()) timing_.lag_kernel_ms = elapsed(lag_events_[0], lag_events_[1]);
     timing_.kernel_launches = launch_counter() - launches0;
 
     auto finish = [&](size_t i) {
@@ -1336,6 +1496,9 @@ void Engine::measure_batch_streamed(size_t n, const double *const *refs, const s
         sum.h2d_bytes += t.h2d_bytes;
         sum.d2h_bytes += t.d2h_bytes;
         sum.host_syncs += t.host_syncs;
+        sum.lag_kernel_ms += t.lag_kernel_ms;
+        sum.lag_bytes += t.lag_bytes;
+        sum.lag_reruns += t.lag_reruns;
     }
     sum.h2d_bytes += h2d;
     timing_ = sum;

@@ -45,11 +45,17 @@ struct PairOutcome {
     PairTrace trace;
 };
 
+// Algorithmic DRAM bytes of one lag search (f32: the FP32 form's search).
+uint64_t lag_search_bytes(const LagJob &j, bool f32);
+
 struct Timing {
     double total_ms = 0, lag_ms = 0, spectrogram_ms = 0, prep_ms = 0, nsim_ms = 0, realign_ms = 0;
     double gammatone_kernel_ms = 0;
     uint64_t gammatone_launches = 0, gammatone_rms = 0, gammatone_window = 0;
     uint64_t kernel_launches = 0, h2d_bytes = 0, d2h_bytes = 0, host_syncs = 0;
+    uint64_t lag_reruns = 0;  // f32 lag searches left undecided and rerun exactly
+    double lag_kernel_ms = 0;  // the global lag search's kernels (events around them)
+    uint64_t lag_bytes = 0;    // their algorithmic DRAM bytes
 };
 
 // Device memory that grows by whole chunks and is recycled per batch.
@@ -57,6 +63,8 @@ class Arena {
 public:
     ~Arena();
     void reset();
+    // Frees every chunk (the device must be done with them).
+    void release();
     void *alloc(size_t bytes);
     template <class T>
     T *alloc_n(size_t n) {
@@ -147,19 +155,30 @@ public:
     // Upper bound on the device memory one pair of these lengths takes in
     // measure_batch (host inputs included), for admission by footprint.
     static size_t pair_footprint(size_t ref_len, size_t deg_len, uint32_t sample_rate, bool speech);
-    // Device memory the engine holds now (arena chunks).
-    size_t reserved_bytes() const { return arena_.reserved(); }
+    // Device memory the engine holds now (arena chunks, upload slots).
+    size_t reserved_bytes() const { return arena_.reserved() + slot_bytes_[0] + slot_bytes_[1]; }
+    // Waits for this engine's work, then frees its arena and upload slots;
+    // the next batch allocates them again.
+    void release_device_memory();
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
 
     // Single-stage entry points (device buffers, exact form).
     void spectrogram(const host::Filterbank &fb, const double *d_hann, size_t window, size_t hop, const double *d_x,
                      size_t len, double *d_out, size_t nf);
-    void lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags);
+    // status_out (optional, njobs): FP32 form, 1 where the f32 search left
+    // the job to the exact one.
+    void lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t *h_lags, int32_t *status_out = nullptr,
+              float *d_corr = nullptr);
+    // The f32 search's nomination and f64 rescoring on a caller-supplied
+    // approximate correlation of raw signals a and b (n values, device),
+    // with the given slack. Returns false when it leaves the lag undecided.
+    bool refine_approx(const VSig &a, const VSig &b, const float *d_approx, int64_t n, double slack, int64_t *lag);
     // FFT twiddles of size n on the device: the full table and the block
     // passes' compact one (cached per size).
     struct Twiddles {
         const double2 *top, *block, *cols, *stages;
+        const float2 *block32, *cols32, *stages32;  // the same tables rounded to f32 (the f32 search)
     };
     Twiddles twiddles(size_t n);
 
@@ -194,8 +213,15 @@ private:
     const RateCache &rate_cache(uint32_t sample_rate);
 
     // Envelope (or raw) lag search for jobs whose a/b/stat pointers are set;
-    // lags land in the jobs' lag_out (device). Launches only.
-    void launch_lag_jobs(std::vector<LagJob> &jobs, bool raw);
+    // lags land in the jobs' lag_out (device). Launches only. The FP32 form
+    // (unless `exact`) runs the f32 search and returns a device array of one
+    // status word per job, in job order: 1 where the f32 search left the job
+    // undecided (its lag_out is untouched); the caller reads it back with the
+    // lags and passes it to rerun_undecided. Else returns null.
+    int32_t *launch_lag_jobs(std::vector<LagJob> &jobs, bool raw, bool exact = false);
+    // The jobs whose status (host copy) is 1, rerun with the exact search;
+    // returns their indices (launches only; nothing when none).
+    std::vector<size_t> rerun_undecided(const std::vector<LagJob> &jobs, const int32_t *h_status, bool raw);
     template <class T>
     T *upload(const std::vector<T> &v);
     void *upload_bytes(const void *src, size_t bytes);
@@ -219,6 +245,7 @@ private:
     cudaStream_t side_ = nullptr;    // reference spectrograms, concurrent with the lag phase
     cudaEvent_t ev_inputs_ = nullptr, ev_ref_done_ = nullptr;
     cudaEvent_t gt_events_[6] = {};  // begin/end of up to three gammatone launches
+    cudaEvent_t lag_events_[2] = {};  // begin/end of the global lag search
     Timing timing_;
     // measure_batch_streamed: copy stream, two upload slots (grow-only
     // device buffers) and the events that mark each slot's upload done.

@@ -30,6 +30,13 @@
 //   over both. All numerator gains go into one f64 factor on the RMS.
 // * the squared outputs are summed in f32 over runs of 16 samples and the
 //   runs are added in f64.
+// * the lowest band group (8 bands) runs all four stages in f64, as the
+//   FP64-FMA form does: its poles sit nearest the unit circle, where f32
+//   state noise grows most, and the spectrogram preparation (per-frame
+//   floors, joint minimum) carries that error into every band. This is the
+//   compensated state such bands need; on this part an f64 stage (3 FMAs on
+//   the half-rate FP64 pipe) costs less than a double-single one (~20 f32
+//   operations).
 //
 // Per frame-sample that is 6 FP64 FMAs (16 lanes per SM sub-partition) and
 // 11-13 FP32 FMAs (32 lanes), which keeps both pipes about equally busy.
@@ -264,9 +271,9 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
         const bool more = i0 + kTileS < window;
         if (more) fetch(i0 + kTileS, buf ^ 1);
         const int count = window - i0 < kTileS ? window - i0 : kTileS;
-        if constexpr (kF64)
+        if (kF64 || k.arith == kArithF64)
             filter_tile64(wx[buf], q, count, k, CA, CB);
-        else if (k.direct_i)
+        else if (k.arith == kArithF32Df1)
             filter_tile<true>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
         else
             filter_tile<false>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
@@ -278,7 +285,7 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
         }
         buf ^= 1;
     }
-    if constexpr (kF64) {
+    if (kF64 || k.arith == kArithF64) {
         acc_a = CA.acc;
         acc_b = CB.acc;
     }
@@ -291,13 +298,13 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
 }
 
 // kThreads = 64 x ceil(nb / 8): 256 for 32 bands, 192 for 21. kCtasPerSm
-// sets the register budget (2: 108 registers at 256 threads, no spills; 3:
-// 80, a few spills; 4: 64, more). kPersistent: a grid of kCtasPerSm CTAs per SM takes tiles
-// from a device-side work queue (an atomic counter over the tile list, zero
-// at launch) instead of one CTA per tile. Both choices are measured by the
-// autotuner; every tile is computed the same either way. kF64: the FP64-FMA
-// form on the same staged tiles (2 CTAs per SM: 128 registers at 256
-// threads).
+// sets the register budget: 2 (128 registers at 256 threads), which the f32
+// form needs since its lowest band group's warps hold the all-f64 cascade
+// (budgets of 3 or 4 CTAs spill over 1 KB a thread). kPersistent: a grid of
+// kCtasPerSm CTAs per SM takes tiles from a device-side work queue (an
+// atomic counter over the tile list, zero at launch) instead of one CTA per
+// tile; every tile is computed the same either way. kF64: the FP64-FMA form
+// on the same staged tiles.
 template <int kThreads, int kCtasPerSm, bool kPersistent, bool kF64 = false>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm * 256 / kThreads) gammatone_fast_kernel(
     const SpecJob *__restrict__ jobs, const Tile *__restrict__ tiles, int ntiles, int *__restrict__ queue,
@@ -411,12 +418,19 @@ __global__ void __launch_bounds__(256, 2) gammatone_f64fma_kernel(const SpecJob 
 int gammatone_fast_frames_per_cta() { return kFramesPerBlock * kBlocksPerCta; }
 
 void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, FastBandCoeffs *out) {
-    // Direct form I for band groups whose highest centre frequency is below
-    // 3 kHz (the exact split is not critical: both forms stay far inside
-    // the fast form's tolerance near the boundary).
+    // The lowest band group runs all four stages in f64: its poles sit
+    // nearest the unit circle (1 - r = 0.004 .. 0.011 at 48 kHz), where f32
+    // state noise is amplified most, and through the per-frame floors and
+    // the joint minimum of the spectrogram preparation that error reaches
+    // every band (with f32 stages there, MOS moved by up to 4e-6 on
+    // low-SNR 48 kHz pairs; with f64 there, by at most 4e-7). Above it,
+    // direct form I for band groups whose highest centre frequency is below
+    // 3 kHz, else the transposed form (the exact split is not critical:
+    // both forms stay far inside the fast form's tolerance near the
+    // boundary).
     for (int g = 0; g * 8 < nb; ++g) {
         const int hi = g * 8 + 7 < nb ? g * 8 + 7 : nb - 1;
-        const int32_t direct_i = cf[hi] < 3000.0 ? 1 : 0;
+        const int32_t arith = g == 0 ? kArithF64 : cf[hi] < 3000.0 ? kArithF32Df1 : kArithF32Df2t;
         for (int b = g * 8; b <= hi; ++b) {
             const BandCoeffs &c = run[b];
             FastBandCoeffs &k = out[b];
@@ -434,18 +448,17 @@ void fill_fast_band_coeffs(const BandCoeffs *run, const double *cf, int nb, Fast
             k.p1l = (float)(c.d1 - (double)k.p1h);
             k.p2h = (float)c.d2;
             k.p2l = (float)(c.d2 - (double)k.p2h);
-            k.direct_i = direct_i;
+            k.arith = arith;
         }
     }
 }
 
 // Launch shapes: CTAs per SM (register budget) + 100 for the persistent
-// work-queue form. The autotuner measures the first three; the persistent
-// shapes measured ~4.5% slower inside the four-lane batch pipeline (their
-// resident CTAs hold SMs the other lanes' kernels would take) and are
-// selected only by VISQOL_TUNE_3.
-std::vector<int> gammatone_fast_shape_candidates() { return {3, 4, 2}; }
-std::vector<int> gammatone_fast_shapes() { return {3, 4, 2, 103, 104}; }
+// work-queue form. The persistent shape measured ~4.5% slower inside the
+// four-lane batch pipeline (its resident CTAs hold SMs the other lanes'
+// kernels would take), so it is selected only by VISQOL_TUNE_3.
+std::vector<int> gammatone_fast_shape_candidates() { return {2}; }
+std::vector<int> gammatone_fast_shapes() { return {2, 102}; }
 
 namespace {
 int sm_count() {
@@ -467,19 +480,11 @@ void launch_gammatone_fast(const SpecJob *d_jobs, const void *d_tiles, int ntile
 #define VQB_FAST(T, C, P)                                                                                    \
     gammatone_fast_kernel<T, C, P><<<grid, T, 0, s>>>(d_jobs, t, ntiles, d_queue, d_coeffs, nb, d_hann, window, \
                                                       hop)
-#define VQB_FAST_T(T)                    \
-    if (persistent) {                    \
-        if (ctas == 4)                   \
-            VQB_FAST(T, 4, true);        \
-        else                             \
-            VQB_FAST(T, 3, true);        \
-    } else if (ctas == 4) {              \
-        VQB_FAST(T, 4, false);           \
-    } else if (ctas == 2) {              \
-        VQB_FAST(T, 2, false);           \
-    } else {                             \
-        VQB_FAST(T, 3, false);           \
-    }
+#define VQB_FAST_T(T)         \
+    if (persistent)           \
+        VQB_FAST(T, 2, true); \
+    else                      \
+        VQB_FAST(T, 2, false);
     if (nb > 24) {
         VQB_FAST_T(256)
     } else if (nb > 16) {

@@ -18,6 +18,24 @@
 //
 // Butterflies and twiddles are those of the radix-2 DIF/DIT (reference
 // src/dsp/fft.zig:127-166); every schedule of them gives the same bits.
+//
+// The passes are written once for two complex types. double2 is the exact
+// search: every product and sum rounded separately, the CPU's results bit
+// for bit. float2 is the FP32 form's search (reference src/xcorr.zig:270-340,
+// its GPU flow src/gpu/engine.zig:445-540): the same schedule in f32 with
+// FMA, half the bytes per pass. Its correlation is within
+// tol(n) n (|a|^2 + |b|^2) of the exact one, tol(n) = 8 eps_f32 log2(n)
+// (src/gpu/engine.zig:820-822), so every lag whose |Re| lies within twice
+// that of the largest is nominated (each inverse CTA keeps those within the
+// slack of its own maximum, a superset), at most kLagCandCap of them per
+// search; they are rescored by f64 dot products of the envelopes and the
+// first maximum in ascending lag wins. A search with more candidates (long
+// runs of near-equal correlation: silence, periodic signals) reports it,
+// and the host reruns it with the exact search.
+#include <algorithm>
+#include <cfloat>
+#include <type_traits>
+
 #include "device.cuh"
 #include "kernels.h"
 
@@ -43,6 +61,33 @@ __device__ inline double2 cross_term(double2 x, double2 zy) {
     const double2 dif_c = make_double2(x.x - y.x, -(x.y - y.y));
     const double2 idc = make_double2(-dif_c.y, dif_c.x);
     return make_double2(0.25 * (sum.x * idc.x - sum.y * idc.y), 0.25 * (sum.x * idc.y + sum.y * idc.x));
+}
+
+// f32: products and sums fused where they chain.
+__device__ inline float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ inline float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ inline float2 cmul(float2 x, float2 w) {
+    return make_float2(__fmaf_rn(x.x, w.x, -(x.y * w.y)), __fmaf_rn(x.x, w.y, x.y * w.x));
+}
+__device__ inline float2 cmul_conj(float2 x, float2 w) {
+    return make_float2(__fmaf_rn(x.x, w.x, x.y * w.y), __fmaf_rn(x.y, w.x, -(x.x * w.y)));
+}
+__device__ inline float2 cross_term(float2 x, float2 zy) {
+    const float2 sum = make_float2(x.x + zy.x, x.y - zy.y);
+    const float2 idc = make_float2(x.y + zy.y, x.x - zy.x);  // i * conj(x - conj(zy))
+    return make_float2(0.25f * __fmaf_rn(sum.x, idc.x, -(sum.y * idc.y)),
+                       0.25f * __fmaf_rn(sum.x, idc.y, sum.y * idc.x));
+}
+
+template <class C>
+__device__ inline C *zbuf(const LagJob &j);
+template <>
+__device__ inline double2 *zbuf<double2>(const LagJob &j) {
+    return j.z;
+}
+template <>
+__device__ inline float2 *zbuf<float2>(const LagJob &j) {
+    return j.z32;
 }
 
 // 16-byte asynchronous global-to-shared copy (both addresses 16-byte aligned).
@@ -88,6 +133,44 @@ __device__ inline double2 packed(const LagJob &job, const EnvParams &pa, const E
     return make_double2(re, im);
 }
 
+// Point i of z in the search's type; the f32 search also sums the squares
+// of the f64 envelope values (its nomination slack scales with them).
+template <class C, bool RAW>
+__device__ inline C pack_point(const LagJob &job, const EnvParams &pa, const EnvParams &pb, int64_t i, double &ea,
+                               double &eb) {
+    const double2 v = packed<RAW>(job, pa, pb, i);
+    if constexpr (std::is_same<C, float2>::value) {
+        ea += v.x * v.x;
+        eb += v.y * v.y;
+        return make_float2((float)v.x, (float)v.y);
+    } else {
+        return v;
+    }
+}
+
+// Sum of a double over the CTA in a fixed order (each warp by shuffles, then
+// the warps in index order), returned to every thread.
+__device__ inline double block_sum(double v) {
+    __shared__ double warp_sum[32];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    __syncthreads();  // warp_sum free (an earlier call may still be reading it)
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += warp_sum[w];
+    return t;
+}
+
+// The f32 forward CTAs' envelope energies, summed.
+template <class C>
+__device__ inline void store_energy(const LagJob &job, double ea, double eb) {
+    if constexpr (std::is_same<C, float2>::value) {
+        ea = block_sum(ea);
+        eb = block_sum(eb);
+        if (threadIdx.x == 0) job.energy[blockIdx.x] = make_double2(ea, eb);
+    }
+}
+
 // G column stages on x[t * cols + c] (t < R = 2^G rows); DIT reverses the
 // stage order. Stage l has span n >> l; the twiddle of the lower point (t, c)
 // is W_{n>>l}^j = top[j << l], j = m * 4096 + c0 + c with m = t mod 2h
@@ -101,23 +184,23 @@ __device__ inline int64_t tcol_off(int G, int l) {
     return (R - (R >> l)) * kB;
 }
 
-template <bool DIT>
-__device__ inline void column_stage2(double2 *x, int G, int l, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+template <class C, bool DIT>
+__device__ inline void column_stage2(C *x, int G, int l, int cols, int64_t c0, const C *__restrict__ tcol) {
     const int R = 1 << G, h = R >> (l + 1);
-    const double2 *tw = tcol + tcol_off(G, l) + c0;
+    const C *tw = tcol + tcol_off(G, l) + c0;
     for (int bf = threadIdx.x; bf < (R >> 1) * cols; bf += blockDim.x) {
         const int pr = bf / cols, c = bf - pr * cols;
         const int m = pr % h;
         const int t = (pr / h) * 2 * h + m;
-        const double2 w = tw[(int64_t)m * kB + c];
-        double2 *pa = x + t * cols + c, *pb = x + (t + h) * cols + c;
-        const double2 a = *pa;
+        const C w = tw[(int64_t)m * kB + c];
+        C *pa = x + t * cols + c, *pb = x + (t + h) * cols + c;
+        const C a = *pa;
         if (!DIT) {
-            const double2 b = *pb;
+            const C b = *pb;
             *pa = cadd(a, b);
             *pb = cmul(csub(a, b), w);
         } else {
-            const double2 b = cmul_conj(*pb, w);
+            const C b = cmul_conj(*pb, w);
             *pa = cadd(a, b);
             *pb = csub(a, b);
         }
@@ -127,19 +210,19 @@ __device__ inline void column_stage2(double2 *x, int G, int l, int cols, int64_t
 // Stages l (span S) and l+1 (span S/2) on 4-row groups t0 + {0,q,2q,3q},
 // q = R >> (l+2): stage l pairs (0,2),(1,3) with twiddle rows m and m+q,
 // stage l+1 pairs (0,1),(2,3) with row m. DIT runs stage l+1 first.
-template <bool DIT>
-__device__ inline void column_stage4(double2 *x, int G, int l, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+template <class C, bool DIT>
+__device__ inline void column_stage4(C *x, int G, int l, int cols, int64_t c0, const C *__restrict__ tcol) {
     const int R = 1 << G, q = R >> (l + 2);
-    const double2 *tw1 = tcol + tcol_off(G, l) + c0, *tw2 = tcol + tcol_off(G, l + 1) + c0;
+    const C *tw1 = tcol + tcol_off(G, l) + c0, *tw2 = tcol + tcol_off(G, l + 1) + c0;
     for (int g = threadIdx.x; g < (R >> 2) * cols; g += blockDim.x) {
         const int pr = g / cols, c = g - pr * cols;
         const int m = pr % q;
         const int t0 = (pr / q) * 4 * q + m;
-        double2 *p0 = x + t0 * cols + c, *p1 = p0 + q * cols, *p2 = p1 + q * cols, *p3 = p2 + q * cols;
-        double2 x0 = *p0, x1 = *p1, x2 = *p2, x3 = *p3;
-        const double2 wa = tw1[(int64_t)m * kB + c], wb = tw1[(int64_t)(m + q) * kB + c];
-        const double2 w2 = tw2[(int64_t)m * kB + c];
-        double2 a, b;
+        C *p0 = x + t0 * cols + c, *p1 = p0 + q * cols, *p2 = p1 + q * cols, *p3 = p2 + q * cols;
+        C x0 = *p0, x1 = *p1, x2 = *p2, x3 = *p3;
+        const C wa = tw1[(int64_t)m * kB + c], wb = tw1[(int64_t)(m + q) * kB + c];
+        const C w2 = tw2[(int64_t)m * kB + c];
+        C a, b;
         if (!DIT) {
             a = x0, b = x2;
             x0 = cadd(a, b);
@@ -171,37 +254,38 @@ __device__ inline void column_stage4(double2 *x, int G, int l, int cols, int64_t
     }
 }
 
-template <bool DIT>
-__device__ inline void column_stages(double2 *x, int G, int cols, int64_t c0, const double2 *__restrict__ tcol) {
+template <class C, bool DIT>
+__device__ inline void column_stages(C *x, int G, int cols, int64_t c0, const C *__restrict__ tcol) {
     if (!DIT) {
         int l = 0;
         for (; l + 1 < G; l += 2) {
-            column_stage4<false>(x, G, l, cols, c0, tcol);
+            column_stage4<C, false>(x, G, l, cols, c0, tcol);
             __syncthreads();
         }
         if (l < G) {
-            column_stage2<false>(x, G, l, cols, c0, tcol);
+            column_stage2<C, false>(x, G, l, cols, c0, tcol);
             __syncthreads();
         }
     } else {
         int l = G - 1;
         if (G & 1) {
-            column_stage2<true>(x, G, l, cols, c0, tcol);
+            column_stage2<C, true>(x, G, l, cols, c0, tcol);
             __syncthreads();
             --l;
         }
         for (; l >= 1; l -= 2) {
-            column_stage4<true>(x, G, l - 1, cols, c0, tcol);
+            column_stage4<C, true>(x, G, l - 1, cols, c0, tcol);
             __syncthreads();
         }
     }
 }
 
 // Pass 1: pack + DIF column stages. grid (n / (R*cols) ... = 4096/cols, jobs).
-template <bool RAW>
+template <class C, bool RAW>
 __global__ void __launch_bounds__(kThreads, 3) fwd_columns(const LagJob *__restrict__ jobs, int G,
-                                                        const double2 *__restrict__ tcol) {
-    extern __shared__ double2 sm[];
+                                                        const C *__restrict__ tcol) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
     const LagJob job = jobs[blockIdx.y];
     const int cols = kB >> G > 0 ? (kB >> G) : 1;
     const int64_t c0 = (int64_t)blockIdx.x * cols;
@@ -212,58 +296,64 @@ __global__ void __launch_bounds__(kThreads, 3) fwd_columns(const LagJob *__restr
     }
     // R * cols = kB points, a fixed 16 per thread: four at a time keeps
     // eight signal loads in flight within the three-CTA register budget.
+    double ea = 0.0, eb = 0.0;
 #pragma unroll 4
     for (int k = 0; k < kB / kThreads; ++k) {
         const int e = threadIdx.x + k * kThreads;
         const int t = e / cols, c = e - t * cols;
-        sm[e] = packed<RAW>(job, pa, pb, (int64_t)t * kB + c0 + c);
+        sm[e] = pack_point<C, RAW>(job, pa, pb, (int64_t)t * kB + c0 + c, ea, eb);
     }
     __syncthreads();
-    column_stages<false>(sm, G, cols, c0, tcol);
+    column_stages<C, false>(sm, G, cols, c0, tcol);
+    C *z = zbuf<C>(job);
 #pragma unroll 4
     for (int k = 0; k < kB / kThreads; ++k) {
         const int e = threadIdx.x + k * kThreads;
         const int t = e / cols, c = e - t * cols;
-        job.z[(int64_t)t * kB + c0 + c] = sm[e];
+        z[(int64_t)t * kB + c0 + c] = sm[e];
     }
+    store_energy<C>(job, ea, eb);
 }
 
 // Radix-4/radix-2 block stages of one B-point block in shared memory
 // (tw[k] = W_B^k); the same stage plans as the stand-alone block passes.
-__device__ inline void dif2(double2 *sm, int B, int s, const double2 *tw) {
+template <class C>
+__device__ inline void dif2(C *sm, int B, int s, const C *tw) {
     const int h = s >> 1, step = B / s;
     for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
         const int blk = bf / h, j = bf - blk * h;
         const int i0 = blk * s + j;
-        const double2 a = sm[i0], b = sm[i0 + h];
+        const C a = sm[i0], b = sm[i0 + h];
         sm[i0] = cadd(a, b);
         sm[i0 + h] = cmul(csub(a, b), tw[j * step]);
     }
 }
-__device__ inline void dit2(double2 *sm, int B, int s, const double2 *tw) {
+template <class C>
+__device__ inline void dit2(C *sm, int B, int s, const C *tw) {
     const int h = s >> 1, step = B / s;
     for (int bf = threadIdx.x; bf < (B >> 1); bf += blockDim.x) {
         const int blk = bf / h, j = bf - blk * h;
         const int i0 = blk * s + j;
-        const double2 a = sm[i0];
-        const double2 b = cmul_conj(sm[i0 + h], tw[j * step]);
+        const C a = sm[i0];
+        const C b = cmul_conj(sm[i0 + h], tw[j * step]);
         sm[i0] = cadd(a, b);
         sm[i0 + h] = csub(a, b);
     }
 }
-__device__ inline void dif4(double2 *sm, int B, int s, const double2 *tw) {
+template <class C>
+__device__ inline void dif4(C *sm, int B, int s, const C *tw) {
     const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
     for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
         const int blk = g / q, j = g - blk * q;
         const int b0 = blk * s + j;
-        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
-        double2 a = x0, b = x2;
+        C x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        C a = x0, b = x2;
         x0 = cadd(a, b);
         x2 = cmul(csub(a, b), tw[j * st1]);
         a = x1, b = x3;
         x1 = cadd(a, b);
         x3 = cmul(csub(a, b), tw[(j + q) * st1]);
-        const double2 w = tw[j * st2];
+        const C w = tw[j * st2];
         a = x0, b = x1;
         x0 = cadd(a, b);
         x1 = cmul(csub(a, b), w);
@@ -273,14 +363,15 @@ __device__ inline void dif4(double2 *sm, int B, int s, const double2 *tw) {
         sm[b0] = x0, sm[b0 + q] = x1, sm[b0 + 2 * q] = x2, sm[b0 + 3 * q] = x3;
     }
 }
-__device__ inline void dit4(double2 *sm, int B, int s, const double2 *tw) {
+template <class C>
+__device__ inline void dit4(C *sm, int B, int s, const C *tw) {
     const int q = s >> 2, st1 = B / s, st2 = 2 * st1;
     for (int g = threadIdx.x; g < (B >> 2); g += blockDim.x) {
         const int blk = g / q, j = g - blk * q;
         const int b0 = blk * s + j;
-        double2 x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
-        const double2 w = tw[j * st2];
-        double2 a = x0, b = cmul_conj(x1, w);
+        C x0 = sm[b0], x1 = sm[b0 + q], x2 = sm[b0 + 2 * q], x3 = sm[b0 + 3 * q];
+        const C w = tw[j * st2];
+        C a = x0, b = cmul_conj(x1, w);
         x0 = cadd(a, b);
         x1 = csub(a, b);
         a = x2, b = cmul_conj(x3, w);
@@ -297,7 +388,8 @@ __device__ inline void dit4(double2 *sm, int B, int s, const double2 *tw) {
 }
 
 // Both blocks' stages advance together (one barrier per stage pair).
-__device__ inline void blocks_dif(double2 *s0, double2 *s1, int B, const double2 *tw) {
+template <class C>
+__device__ inline void blocks_dif(C *s0, C *s1, int B, const C *tw) {
     int stages = 0;
     for (int r = B; r > 1; r >>= 1) ++stages;
     int s = B;
@@ -312,7 +404,8 @@ __device__ inline void blocks_dif(double2 *s0, double2 *s1, int B, const double2
         __syncthreads();
     }
 }
-__device__ inline void blocks_dit(double2 *s0, double2 *s1, int B, const double2 *tw) {
+template <class C>
+__device__ inline void blocks_dit(C *s0, C *s1, int B, const C *tw) {
     int stages = 0;
     for (int r = B; r > 1; r >>= 1) ++stages;
     int s = 4;
@@ -348,45 +441,47 @@ constexpr int kPadB = kB + kB / 16;
 
 __device__ inline int padi(int e) { return e + (e >> 4); }
 
-template <int S0>
-__device__ inline void dif16(double2 (&x)[16], int j, const double2 *__restrict__ tst) {
+template <class C, int S0>
+__device__ inline void dif16(C (&x)[16], int j, const C *__restrict__ tst) {
     constexpr int q = S0 / 16;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int half = 8 >> r;
-        const double2 *tw = tst + (kB - (S0 >> r));
+        const C *tw = tst + (kB - (S0 >> r));
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const double2 w = __ldg(tw + j + (m & (half - 1)) * q);
-            const double2 a = x[m], b = x[m + half];
+            const C w = __ldg(tw + j + (m & (half - 1)) * q);
+            const C a = x[m], b = x[m + half];
             x[m] = cadd(a, b);
             x[m + half] = cmul(csub(a, b), w);
         }
     }
 }
 
-template <int S0>
-__device__ inline void dit16(double2 (&x)[16], int j, const double2 *__restrict__ tst) {
+template <class C, int S0>
+__device__ inline void dit16(C (&x)[16], int j, const C *__restrict__ tst) {
     constexpr int q = S0 / 16;
 #pragma unroll
     for (int r = 3; r >= 0; --r) {
         const int half = 8 >> r;
-        const double2 *tw = tst + (kB - (S0 >> r));
+        const C *tw = tst + (kB - (S0 >> r));
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const double2 w = __ldg(tw + j + (m & (half - 1)) * q);
-            const double2 a = x[m], b = cmul_conj(x[m + half], w);
+            const C w = __ldg(tw + j + (m & (half - 1)) * q);
+            const C a = x[m], b = cmul_conj(x[m + half], w);
             x[m] = cadd(a, b);
             x[m + half] = csub(a, b);
         }
     }
 }
 
+template <class C>
 __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__restrict__ jobs,
-                                                                const double2 *__restrict__ tst) {
-    extern __shared__ double2 sm[];
+                                                                const C *__restrict__ tst) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
     const LagJob job = jobs[blockIdx.y];
     const int k = blockIdx.x;
     int64_t b0 = 0, b1 = -1;
@@ -401,14 +496,14 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     }
     const int half = threadIdx.x >> 8, t = threadIdx.x & 255;
     const bool active = half == 0 || b1 >= 0;
-    double2 *own = sm + half * kPadB;
-    double2 *z = job.z + (half == 1 && b1 >= 0 ? b1 : b0) * kB;
-    double2 x[16];
+    C *own = sm + half * kPadB;
+    C *z = zbuf<C>(job) + (half == 1 && b1 >= 0 ? b1 : b0) * kB;
+    C x[16];
     // DIF spans 4096 .. 512: points t + 256 m
     if (active) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = z[t + 256 * m];
-        dif16<4096>(x, t, tst);
+        dif16<C, 4096>(x, t, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) own[padi(t + 256 * m)] = x[m];
     }
@@ -418,7 +513,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     if (active) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = own[padi(base2 + 16 * m)];
-        dif16<256>(x, t & 15, tst);
+        dif16<C, 256>(x, t & 15, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) own[padi(base2 + 16 * m)] = x[m];
     }
@@ -427,7 +522,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     if (active) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = own[padi(16 * t + m)];
-        dif16<16>(x, 0, tst);
+        dif16<C, 16>(x, 0, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) own[padi(16 * t + m)] = x[m];
     }
@@ -437,7 +532,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int u = 16 * t + m;
-            double2 zp;
+            C zp;
             if (b1 >= 0) {
                 zp = sm[(1 - half) * kPadB + padi(kB - 1 - u)];
             } else if (k == 1) {
@@ -456,7 +551,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     __syncthreads();
     // DIT spans 2 .. 16, then 32 .. 256, then 512 .. 4096 (to global memory)
     if (active) {
-        dit16<16>(x, 0, tst);
+        dit16<C, 16>(x, 0, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) own[padi(16 * t + m)] = x[m];
     }
@@ -464,7 +559,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     if (active) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = own[padi(base2 + 16 * m)];
-        dit16<256>(x, t & 15, tst);
+        dit16<C, 256>(x, t & 15, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) own[padi(base2 + 16 * m)] = x[m];
     }
@@ -472,7 +567,7 @@ __global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__
     if (active) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = own[padi(t + 256 * m)];
-        dit16<4096>(x, t, tst);
+        dit16<C, 4096>(x, t, tst);
 #pragma unroll
         for (int m = 0; m < 16; ++m) z[t + 256 * m] = x[m];
     }
@@ -513,7 +608,8 @@ __device__ inline void block_best(Best best, double *pv, int64_t *pk, int64_t sl
 __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__restrict__ jobs, int G,
                                                                const double2 *__restrict__ tcol, double *pv,
                                                                int64_t *pk, int parts) {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *sm = reinterpret_cast<double2 *>(smem_raw);
     const LagJob job = jobs[blockIdx.y];
     const int cols = kB >> G > 0 ? (kB >> G) : 1;
     const int64_t c0 = (int64_t)blockIdx.x * cols;
@@ -528,7 +624,7 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
-    column_stages<true>(sm, G, cols, c0, tcol);
+    column_stages<double2, true>(sm, G, cols, c0, tcol);
     const int64_t n = job.n, max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
     for (int e = threadIdx.x; e < kB; e += blockDim.x) {
@@ -553,25 +649,25 @@ __global__ void __launch_bounds__(kThreads) inv_columns_argmax(const LagJob *__r
 // (stage l, lower row t: tcol[off(l) + (t mod 2h) 4096 + col]), so the
 // results are the same bits; a group costs one barrier instead of one per
 // stage pair.
-template <int G, bool DIT>
-__device__ inline void column_group4(double2 (&x)[16], int l0, int stride, int base_mod,
-                                     const double2 *__restrict__ tcol, int64_t col) {
+template <class C, int G, bool DIT>
+__device__ inline void column_group4(C (&x)[16], int l0, int stride, int base_mod, const C *__restrict__ tcol,
+                                     int64_t col) {
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
         const int k = DIT ? 3 - kk : kk;
         const int l = l0 + k, half = 8 >> k;
-        const double2 *tw = tcol + tcol_off(G, l) + col;
+        const C *tw = tcol + tcol_off(G, l) + col;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const double2 w = __ldg(tw + (int64_t)(base_mod + stride * (m & (half - 1))) * kB);
-            const double2 a = x[m];
+            const C w = __ldg(tw + (int64_t)(base_mod + stride * (m & (half - 1))) * kB);
+            const C a = x[m];
             if (!DIT) {
-                const double2 b = x[m + half];
+                const C b = x[m + half];
                 x[m] = cadd(a, b);
                 x[m + half] = cmul(csub(a, b), w);
             } else {
-                const double2 b = cmul_conj(x[m + half], w);
+                const C b = cmul_conj(x[m + half], w);
                 x[m] = cadd(a, b);
                 x[m + half] = csub(a, b);
             }
@@ -581,26 +677,26 @@ __device__ inline void column_group4(double2 (&x)[16], int l0, int stride, int b
 
 // Stages l0 .. G-1, whose spans h = R >> (l+1) are at most 8, on rows
 // 16 q + m (t mod 2h = m mod 2h).
-template <int G, bool DIT>
-__device__ inline void column_tail(double2 (&x)[16], int l0, const double2 *__restrict__ tcol, int64_t col) {
+template <class C, int G, bool DIT>
+__device__ inline void column_tail(C (&x)[16], int l0, const C *__restrict__ tcol, int64_t col) {
     constexpr int R = 1 << G;
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
         const int l = DIT ? G - 1 - kk : l0 + kk;
         if (l < l0 || l >= G) continue;
         const int h = R >> (l + 1);
-        const double2 *tw = tcol + tcol_off(G, l) + col;
+        const C *tw = tcol + tcol_off(G, l) + col;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & h) continue;
-            const double2 w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
-            const double2 a = x[m];
+            const C w = __ldg(tw + (int64_t)(m & (h - 1)) * kB);
+            const C a = x[m];
             if (!DIT) {
-                const double2 b = x[m + h];
+                const C b = x[m + h];
                 x[m] = cadd(a, b);
                 x[m + h] = cmul(csub(a, b), w);
             } else {
-                const double2 b = cmul_conj(x[m + h], w);
+                const C b = cmul_conj(x[m + h], w);
                 x[m] = cadd(a, b);
                 x[m + h] = csub(a, b);
             }
@@ -618,10 +714,11 @@ __device__ inline int row_b(int q, int m) {
 }
 __device__ inline int row_t(int q, int m) { return 16 * q + m; }
 
-template <int G, bool RAW>
+template <class C, int G, bool RAW>
 __global__ void __launch_bounds__(kThreads, 2) fwd_columns_reg(const LagJob *__restrict__ jobs,
-                                                            const double2 *__restrict__ tcol) {
-    extern __shared__ double2 sm[];
+                                                            const C *__restrict__ tcol) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
     constexpr int R = 1 << G, cols = kB >> G;
     const LagJob job = jobs[blockIdx.y];
     const int c = threadIdx.x % cols, q = threadIdx.x / cols;
@@ -631,10 +728,12 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_columns_reg(const LagJob *__r
         pa = env_params(job.a, job.stats_a);
         pb = env_params(job.b, job.stats_b);
     }
-    double2 x[16];
+    C x[16];
+    double ea = 0.0, eb = 0.0;
 #pragma unroll
-    for (int m = 0; m < 16; ++m) x[m] = packed<RAW>(job, pa, pb, (int64_t)row_a<G>(q, m) * kB + col);
-    column_group4<G, false>(x, 0, R / 16, q, tcol, col);
+    for (int m = 0; m < 16; ++m) x[m] = pack_point<C, RAW>(job, pa, pb, (int64_t)row_a<G>(q, m) * kB + col, ea, eb);
+    column_group4<C, G, false>(x, 0, R / 16, q, tcol, col);
+    C *z = zbuf<C>(job);
     if (G > 4) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) sm[row_a<G>(q, m) * cols + c] = x[m];
@@ -643,27 +742,29 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_columns_reg(const LagJob *__r
             constexpr int s = R / 256 > 0 ? R / 256 : 1;
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
-            column_group4<G, false>(x, 4, s, q % s, tcol, col);
+            column_group4<C, G, false>(x, 4, s, q % s, tcol, col);
 #pragma unroll
             for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
             __syncthreads();
         }
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = sm[row_t(q, m) * cols + c];
-        column_tail<G, false>(x, G > 8 ? 8 : 4, tcol, col);
+        column_tail<C, G, false>(x, G > 8 ? 8 : 4, tcol, col);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) job.z[(int64_t)row_t(q, m) * kB + col] = x[m];
+        for (int m = 0; m < 16; ++m) z[(int64_t)row_t(q, m) * kB + col] = x[m];
     } else {
 #pragma unroll
-        for (int m = 0; m < 16; ++m) job.z[(int64_t)row_a<G>(q, m) * kB + col] = x[m];
+        for (int m = 0; m < 16; ++m) z[(int64_t)row_a<G>(q, m) * kB + col] = x[m];
     }
+    store_energy<C>(job, ea, eb);
 }
 
 template <int G>
 __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__restrict__ jobs,
                                                             const double2 *__restrict__ tcol, double *pv,
                                                             int64_t *pk, int parts) {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *sm = reinterpret_cast<double2 *>(smem_raw);
     constexpr int R = 1 << G, cols = kB >> G;
     const LagJob job = jobs[blockIdx.y];
     const int c = threadIdx.x % cols, q = threadIdx.x / cols;
@@ -672,7 +773,7 @@ __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__r
     if (G > 4) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)row_t(q, m) * kB + col];
-        column_tail<G, true>(x, G > 8 ? 8 : 4, tcol, col);
+        column_tail<double2, G, true>(x, G > 8 ? 8 : 4, tcol, col);
 #pragma unroll
         for (int m = 0; m < 16; ++m) sm[row_t(q, m) * cols + c] = x[m];
         __syncthreads();
@@ -680,7 +781,7 @@ __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__r
             constexpr int s = R / 256 > 0 ? R / 256 : 1;
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
-            column_group4<G, true>(x, 4, s, q % s, tcol, col);
+            column_group4<double2, G, true>(x, 4, s, q % s, tcol, col);
 #pragma unroll
             for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
             __syncthreads();
@@ -691,7 +792,7 @@ __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__r
 #pragma unroll
         for (int m = 0; m < 16; ++m) x[m] = job.z[(int64_t)row_a<G>(q, m) * kB + col];
     }
-    column_group4<G, true>(x, 0, R / 16, q, tcol, col);
+    column_group4<double2, G, true>(x, 0, R / 16, q, tcol, col);
     const int64_t n = job.n, max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
 #pragma unroll
@@ -706,7 +807,8 @@ __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__r
 template <bool RAW>
 __global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__ jobs, const double2 *__restrict__ tw,
                                                       double *pv, int64_t *pk) {
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *sm = reinterpret_cast<double2 *>(smem_raw);
     const LagJob job = jobs[blockIdx.y];
     const int B = (int)job.n;
     EnvParams pa{}, pb{};
@@ -716,7 +818,7 @@ __global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__
     }
     for (int u = threadIdx.x; u < B; u += blockDim.x) sm[u] = packed<RAW>(job, pa, pb, u);
     __syncthreads();
-    blocks_dif(sm, nullptr, B, tw);
+    blocks_dif<double2>(sm, nullptr, B, tw);
     for (int i = threadIdx.x; i < (B > 1 ? B / 2 : 1); i += blockDim.x) {
         if (i == 0) {
             sm[0] = cross_term(sm[0], sm[0]);
@@ -731,7 +833,7 @@ __global__ void __launch_bounds__(kThreads) small_lag(const LagJob *__restrict__
         sm[b] = cross_term(zb, za);
     }
     __syncthreads();
-    blocks_dit(sm, nullptr, B, tw);
+    blocks_dit<double2>(sm, nullptr, B, tw);
     const int64_t max_lag = job.biggest - 1;
     Best best{-INFINITY, INT64_MAX};
     for (int u = threadIdx.x; u < B; u += blockDim.x) {
@@ -757,16 +859,327 @@ __global__ void pick_lag(const LagJob *__restrict__ jobs, int njobs, const doubl
     if (lane == 0) *jobs[j].lag_out = best.key == INT64_MAX ? 0 : best.key - (jobs[j].biggest - 1);
 }
 
+// ---- f32 search: nomination, pick, f64 rescoring ---------------------------
+
+// Twice the f32 correlation's error bound, 2 tol(n) n (|a|^2 + |b|^2) with
+// tol(n) = 8 eps_f32 log2(n) (reference refineSlack src/xcorr.zig:302-308,
+// lagTolerance src/gpu/engine.zig:820-822), from the forward CTAs' energy
+// sums. Every thread gets the same value (a fixed summation order).
+__device__ inline double job_slack(const LagJob &job, int parts) {
+    if (job.slack_fixed > 0.0) return job.slack_fixed;
+    double e = 0.0;
+    for (int p = threadIdx.x; p < parts; p += blockDim.x) e += job.energy[p].x + job.energy[p].y;
+    e = block_sum(e);
+    int lg = 0;
+    for (int64_t r = job.n; r > 1; r >>= 1) ++lg;
+    const double tol = 8.0 * (double)FLT_EPSILON * (double)lg;
+    return 2.0 * tol * e * (double)job.n;
+}
+
+__device__ inline float block_max(float v) {
+    __shared__ float warp_max[32];
+    for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, off));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float t = -INFINITY;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, warp_max[w]);
+    return t;
+}
+
+// This CTA's nomination record: its largest |Re| over valid lags (key >= 0)
+// and every lag within `slack` of it (a superset of the search's candidates
+// here, since the search's largest is at least this CTA's).
+__device__ inline void block_nominate(const float (&v)[16], const int32_t (&key)[16], double slack, LagCands *out) {
+    float top = -INFINITY;
+#pragma unroll
+    for (int m = 0; m < 16; ++m)
+        if (key[m] >= 0) top = fmaxf(top, v[m]);
+    top = block_max(top);
+    __shared__ int count;
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    const double floor = (double)top - slack;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        if (key[m] >= 0 && (double)v[m] >= floor) {
+            const int i = atomicAdd(&count, 1);
+            if (i < kLagCandCap) {
+                out->v[i] = v[m];
+                out->key[i] = key[m];
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out->top = top;
+        out->count = count;
+    }
+}
+
+// 8-byte asynchronous global-to-shared copy (both addresses 8-byte aligned).
+__device__ inline void cp_async8(float2 *dst, const float2 *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Pass 3 of the f32 search, shared-memory column form (any G): DIT column
+// stages, then this CTA's nomination record. parts: CTAs per job.
+__global__ void __launch_bounds__(kThreads) inv_columns_nominate(const LagJob *__restrict__ jobs, int G,
+                                                                 const float2 *__restrict__ tcol, int parts) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *sm = reinterpret_cast<float2 *>(smem_raw);
+    const LagJob job = jobs[blockIdx.y];
+    const int cols = kB >> G > 0 ? (kB >> G) : 1;
+    const int64_t c0 = (int64_t)blockIdx.x * cols;
+#pragma unroll
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
+        const int t = e / cols, c = e - t * cols;
+        cp_async8(sm + e, job.z32 + (int64_t)t * kB + c0 + c);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    column_stages<float2, true>(sm, G, cols, c0, tcol);
+    const double slack = job_slack(job, parts);
+    const int64_t n = job.n, max_lag = job.biggest - 1;
+    float v[16];
+    int32_t key[16];
+#pragma unroll
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
+        const int t = e / cols, c = e - t * cols;
+        const int64_t i = (int64_t)t * kB + c0 + c;
+        v[k] = fabsf(sm[e].x);
+        key[k] = (int32_t)lag_key(i, n, max_lag);
+        if (job.corr_out) job.corr_out[i] = sm[e].x;
+    }
+    block_nominate(v, key, slack, job.cands + blockIdx.x);
+}
+
+// Pass 3 of the f32 search, register form (4 <= G <= 11).
+template <int G>
+__global__ void __launch_bounds__(kThreads, 2) inv_columns_reg_nominate(const LagJob *__restrict__ jobs,
+                                                                     const float2 *__restrict__ tcol, int parts) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *sm = reinterpret_cast<float2 *>(smem_raw);
+    constexpr int R = 1 << G, cols = kB >> G;
+    const LagJob job = jobs[blockIdx.y];
+    const int c = threadIdx.x % cols, q = threadIdx.x / cols;
+    const int64_t col = (int64_t)blockIdx.x * cols + c;
+    float2 x[16];
+    if (G > 4) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = job.z32[(int64_t)row_t(q, m) * kB + col];
+        column_tail<float2, G, true>(x, G > 8 ? 8 : 4, tcol, col);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) sm[row_t(q, m) * cols + c] = x[m];
+        __syncthreads();
+        if (G > 8) {
+            constexpr int s = R / 256 > 0 ? R / 256 : 1;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
+            column_group4<float2, G, true>(x, 4, s, q % s, tcol, col);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[row_a<G>(q, m) * cols + c];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = job.z32[(int64_t)row_a<G>(q, m) * kB + col];
+    }
+    column_group4<float2, G, true>(x, 0, R / 16, q, tcol, col);
+    const double slack = job_slack(job, parts);
+    const int64_t n = job.n, max_lag = job.biggest - 1;
+    float v[16];
+    int32_t key[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int64_t i = (int64_t)row_a<G>(q, m) * kB + col;
+        v[m] = fabsf(x[m].x);
+        key[m] = (int32_t)lag_key(i, n, max_lag);
+        if (job.corr_out) job.corr_out[i] = x[m].x;
+    }
+    block_nominate(v, key, slack, job.cands + blockIdx.x);
+}
+
+// n <= 4096: the whole f32 search's transform and nomination in one CTA.
+template <bool RAW>
+__global__ void __launch_bounds__(kThreads) small_lag32(const LagJob *__restrict__ jobs, const float2 *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *sm = reinterpret_cast<float2 *>(smem_raw);
+    const LagJob job = jobs[blockIdx.y];
+    const int B = (int)job.n;
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    double ea = 0.0, eb = 0.0;
+    for (int u = threadIdx.x; u < B; u += blockDim.x) sm[u] = pack_point<float2, RAW>(job, pa, pb, u, ea, eb);
+    ea = block_sum(ea);
+    eb = block_sum(eb);
+    if (threadIdx.x == 0) job.energy[0] = make_double2(ea, eb);
+    __syncthreads();
+    blocks_dif<float2>(sm, nullptr, B, tw);
+    for (int i = threadIdx.x; i < (B > 1 ? B / 2 : 1); i += blockDim.x) {
+        if (i == 0) {
+            sm[0] = cross_term(sm[0], sm[0]);
+            if (B > 1) sm[1] = cross_term(sm[1], sm[1]);
+            continue;
+        }
+        const int p = 1 << (31 - __clz(i));
+        const int h = 2 * p;
+        const int a = i + p, b = 3 * h - 1 - a;
+        const float2 za = sm[a], zb = sm[b];
+        sm[a] = cross_term(za, zb);
+        sm[b] = cross_term(zb, za);
+    }
+    __syncthreads();
+    blocks_dit<float2>(sm, nullptr, B, tw);
+    const double slack = job_slack(job, 1);
+    const int64_t max_lag = job.biggest - 1;
+    float v[16];
+    int32_t key[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int u = threadIdx.x + k * kThreads;
+        key[k] = -1;
+        v[k] = 0.f;
+        if (u < B) {
+            v[k] = fabsf(sm[u].x);
+            key[k] = (int32_t)lag_key(u, B, max_lag);
+            if (job.corr_out) job.corr_out[u] = sm[u].x;
+        }
+    }
+    block_nominate(v, key, slack, job.cands);
+}
+
+// Nomination records of an approximate correlation supplied by the caller
+// (approx = corr_out, n values, circular index order), 4096 values a CTA:
+// the reference's refineLag input (src/xcorr.zig:278-300). grid (parts, 1).
+__global__ void __launch_bounds__(kThreads) nominate_approx(const LagJob *__restrict__ jobs) {
+    const LagJob job = jobs[0];
+    const int64_t n = job.n, max_lag = job.biggest - 1;
+    float v[16];
+    int32_t key[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int64_t i = (int64_t)blockIdx.x * kB + threadIdx.x + k * kThreads;
+        key[k] = -1;
+        v[k] = 0.f;
+        if (i < n) {
+            v[k] = fabsf(job.corr_out[i]);
+            key[k] = (int32_t)lag_key(i, n, max_lag);
+        }
+    }
+    block_nominate(v, key, job.slack_fixed, job.cands + blockIdx.x);
+}
+
+// The search's candidates: lags whose |Re| is within the slack of the
+// largest (reference refineLag src/xcorr.zig:278-300), from the CTAs'
+// records. Over kLagCandCap of them, or a CTA near the top whose own list
+// overflowed, sets status 1 (the exact search decides). One CTA per job.
+__global__ void __launch_bounds__(kThreads) pick_candidates(const LagJob *__restrict__ jobs, int parts) {
+    const LagJob job = jobs[blockIdx.x];
+    const double slack = job_slack(job, parts);
+    float top = -INFINITY;
+    for (int p = threadIdx.x; p < parts; p += blockDim.x) top = fmaxf(top, job.cands[p].top);
+    top = block_max(top);
+    const double floor = (double)top - slack;
+    __shared__ int count, over;
+    if (threadIdx.x == 0) count = 0, over = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < parts; p += blockDim.x) {
+        const LagCands &c = job.cands[p];
+        if ((double)c.top < floor) continue;
+        if (c.count > kLagCandCap) {
+            over = 1;
+            continue;
+        }
+        for (int i = 0; i < c.count; ++i) {
+            if ((double)c.v[i] < floor) continue;
+            const int k = atomicAdd(&count, 1);
+            if (k < kLagCandCap) job.cand_key[k] = c.key[i];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int bad = over || count > kLagCandCap || count == 0;
+        *job.status = bad;
+        *job.ncand = bad ? 0 : count;
+    }
+}
+
+constexpr int kRescoreChunk = 4096;  // b samples per rescoring CTA
+
+// Partial dot products sum_j a[j + lag] b[j] of every candidate lag over
+// this CTA's chunk of b (reference dotAtLag src/xcorr.zig:328-340; the
+// summation order is this kernel's, fixed), of the envelopes (or raw
+// signals), in f64. grid (chunks, jobs).
+template <bool RAW>
+__global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__restrict__ jobs, int nchunks) {
+    const LagJob job = jobs[blockIdx.y];
+    if (*job.status != 0) return;
+    const int count = *job.ncand;
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    const int64_t max_lag = job.biggest - 1;
+    const int64_t j0 = (int64_t)blockIdx.x * kRescoreChunk;
+    for (int c = 0; c < count; ++c) {
+        const int64_t lag = (int64_t)job.cand_key[c] - max_lag;
+        double acc = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < kRescoreChunk / kThreads; ++k) {
+            const int64_t j = j0 + threadIdx.x + k * kThreads, ia = j + lag;
+            if (j < job.b.len && ia >= 0 && ia < job.a.len) {
+                const double x = RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia);
+                const double y = RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j);
+                acc += x * y;
+            }
+        }
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) job.rescore[(int64_t)c * nchunks + blockIdx.x] = acc;
+    }
+}
+
+// The first maximum of |dot| in ascending lag (reference rescore
+// src/xcorr.zig:311-325). One warp per job.
+__global__ void pick_rescored(const LagJob *__restrict__ jobs, int njobs, int nchunks) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (j >= njobs) return;
+    const LagJob job = jobs[j];
+    if (*job.status != 0) return;
+    const int count = *job.ncand;
+    Best best{-INFINITY, INT64_MAX};
+    for (int c = lane; c < count; c += 32) {
+        double d = 0.0;
+        for (int k = 0; k < nchunks; ++k) d += job.rescore[(int64_t)c * nchunks + k];
+        best = better(best, Best{fabs(d), (int64_t)job.cand_key[c]});
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        Best o{__shfl_down_sync(0xffffffffu, best.v, off), __shfl_down_sync(0xffffffffu, best.key, off)};
+        best = better(best, o);
+    }
+    if (lane == 0) *job.lag_out = best.key - (job.biggest - 1);
+}
+
 }  // namespace
 
 void lag_init_attributes() {
     const int one = kB * (int)sizeof(double2);
-    cudaFuncSetAttribute(fwd_columns<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
-    cudaFuncSetAttribute(fwd_columns<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(fwd_columns<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(fwd_columns<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(inv_columns_argmax, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
-#define VQB_COLS_ATTR(GG)                                                                        \
-    cudaFuncSetAttribute(fwd_columns_reg<GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);  \
-    cudaFuncSetAttribute(fwd_columns_reg<GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+#define VQB_COLS_ATTR(GG)                                                                                 \
+    cudaFuncSetAttribute(fwd_columns_reg<double2, GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);  \
+    cudaFuncSetAttribute(fwd_columns_reg<double2, GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
     cudaFuncSetAttribute(inv_columns_reg<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     VQB_COLS_ATTR(5)
     VQB_COLS_ATTR(6)
@@ -778,7 +1191,7 @@ void lag_init_attributes() {
 #undef VQB_COLS_ATTR
     cudaFuncSetAttribute(small_lag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
     cudaFuncSetAttribute(small_lag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
-    cudaFuncSetAttribute(middle_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(middle_blocks<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(2 * kPadB * sizeof(double2)));
 }
 
@@ -841,9 +1254,9 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
 #define VQB_COLS(GG)                                                                                       \
     case GG:                                                                                               \
         if (raw)                                                                                           \
-            fwd_columns_reg<GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);                      \
+            fwd_columns_reg<double2, GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);             \
         else                                                                                               \
-            fwd_columns_reg<GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);                     \
+            fwd_columns_reg<double2, GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);            \
         break;
         VQB_COLS(4)
         VQB_COLS(5)
@@ -856,11 +1269,11 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
 #undef VQB_COLS
     default:
         if (raw)
-            fwd_columns<true><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+            fwd_columns<double2, true><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
         else
-            fwd_columns<false><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+            fwd_columns<double2, false><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
     }
-    middle_blocks<<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads, 2 * kPadB * sizeof(double2), s>>>(
+    middle_blocks<double2><<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads, 2 * kPadB * sizeof(double2), s>>>(
         d_jobs, tst);
     switch (Gr) {
 #define VQB_COLS(GG)                                                                                       \
@@ -881,6 +1294,104 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
     }
     pick_lag<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, pv, pk, parts);
     launch_counter() += 4;
+}
+
+void launch_refine_approx(const LagJob *d_job, int64_t n, int nchunks, cudaStream_t s) {
+    const int parts = (int)((n + kB - 1) / kB);
+    nominate_approx<<<parts, kThreads, 0, s>>>(d_job);
+    pick_candidates<<<1, kThreads, 0, s>>>(d_job, parts);
+    rescore_candidates<true><<<dim3((unsigned)nchunks, 1), kThreads, 0, s>>>(d_job, nchunks);
+    pick_rescored<<<1, 32, 0, s>>>(d_job, 1, nchunks);
+    launch_counter() += 4;
+}
+
+void lag32_init_attributes() {
+    const int one = kB * (int)sizeof(float2);
+    cudaFuncSetAttribute(fwd_columns<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(fwd_columns<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(inv_columns_nominate, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(small_lag32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(small_lag32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    cudaFuncSetAttribute(middle_blocks<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(2 * kPadB * sizeof(float2)));
+}
+
+size_t lag32_parts(int64_t n) { return n <= kB ? 1 : fused_lag_parts(n); }
+
+int lag32_rescore_chunks(int64_t max_b_len) {
+    return (int)std::max<int64_t>(1, (max_b_len + kRescoreChunk - 1) / kRescoreChunk);
+}
+
+void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const float2 *tcol, const float2 *tw_block,
+                  const float2 *tst, int nchunks, cudaStream_t s) {
+    if (njobs <= 0) return;
+    const int parts = (int)lag32_parts(n);
+    if (n <= kB) {
+        const size_t smem = (size_t)n * sizeof(float2);
+        if (raw)
+            small_lag32<true><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block);
+        else
+            small_lag32<false><<<dim3(1, (unsigned)njobs), kThreads, smem, s>>>(d_jobs, tw_block);
+        launch_counter() += 1;
+    } else {
+        int G = 0;
+        for (int64_t r = n / kB; r > 1; r >>= 1) ++G;
+        const int64_t nblk = n / kB;
+        const dim3 grid((unsigned)parts, (unsigned)njobs);
+        const size_t one = (size_t)kB * sizeof(float2);
+        const size_t reg_smem = G > 4 ? one : 0;
+        const int Gr = fused_lag_register_columns(n) ? G : 0;
+        switch (Gr) {
+#define VQB_COLS32(GG)                                                                                     \
+    case GG:                                                                                               \
+        if (raw)                                                                                           \
+            fwd_columns_reg<float2, GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);              \
+        else                                                                                               \
+            fwd_columns_reg<float2, GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);             \
+        break;
+            VQB_COLS32(4)
+            VQB_COLS32(5)
+            VQB_COLS32(6)
+            VQB_COLS32(7)
+            VQB_COLS32(8)
+            VQB_COLS32(9)
+            VQB_COLS32(10)
+            VQB_COLS32(11)
+#undef VQB_COLS32
+        default:
+            if (raw)
+                fwd_columns<float2, true><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+            else
+                fwd_columns<float2, false><<<grid, kThreads, one, s>>>(d_jobs, G, tcol);
+        }
+        middle_blocks<float2><<<dim3((unsigned)(nblk / 2 + 1), (unsigned)njobs), kMidThreads,
+                                2 * kPadB * sizeof(float2), s>>>(d_jobs, tst);
+        switch (Gr) {
+#define VQB_COLS32(GG)                                                                                     \
+    case GG:                                                                                               \
+        inv_columns_reg_nominate<GG><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol, parts);               \
+        break;
+            VQB_COLS32(4)
+            VQB_COLS32(5)
+            VQB_COLS32(6)
+            VQB_COLS32(7)
+            VQB_COLS32(8)
+            VQB_COLS32(9)
+            VQB_COLS32(10)
+            VQB_COLS32(11)
+#undef VQB_COLS32
+        default:
+            inv_columns_nominate<<<grid, kThreads, one, s>>>(d_jobs, G, tcol, parts);
+        }
+        launch_counter() += 3;
+    }
+    pick_candidates<<<njobs, kThreads, 0, s>>>(d_jobs, parts);
+    if (raw)
+        rescore_candidates<true><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
+    else
+        rescore_candidates<false><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
+    pick_rescored<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, nchunks);
+    launch_counter() += 3;
 }
 
 }  // namespace vqb

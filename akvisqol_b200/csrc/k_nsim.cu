@@ -12,6 +12,8 @@
 // Interior patch columns reuse the plane's terms, whose 3x3 neighbourhood
 // is the patch's; the two edge columns are recomputed with the patch's
 // replicate padding, as the CPU does.
+#include <algorithm>
+
 #include "device.cuh"
 #include "kernels.h"
 
@@ -402,6 +404,13 @@ __global__ void __launch_bounds__(32) stats_kernel(const StatsJob *__restrict__ 
     }
 }
 
+// fast_quotient over arrays (its direct test against IEEE division).
+__global__ void quotient_kernel(const double *__restrict__ num, const double *__restrict__ den,
+                                double *__restrict__ out, size_t count) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = fast_quotient(num[i], den[i]);
+}
+
 }  // namespace
 
 void launch_plane(const PlaneJob *d_jobs, int njobs, int nb, int max_width, cudaStream_t s) {
@@ -493,6 +502,13 @@ void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast
         VQB_TABLE(128)
     }
 #undef VQB_TABLE
+    launch_counter() += 1;
+}
+
+void launch_fast_quotient(const double *num, const double *den, double *out, size_t count, cudaStream_t s) {
+    if (count == 0) return;
+    const size_t blocks = std::min<size_t>((count + 255) / 256, 4096);
+    quotient_kernel<<<(unsigned)blocks, 256, 0, s>>>(num, den, out, count);
     launch_counter() += 1;
 }
 

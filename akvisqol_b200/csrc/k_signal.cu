@@ -48,9 +48,10 @@ __device__ inline void tile_terms(double v, int64_t k, double mean, double &t0, 
 // tiles: this warp's 2 (buffers) x 2 (chains) x kTile doubles.
 template <int KIND>
 __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, double mean, double &acc0,
-                                   double &acc1, double *tiles) {
+                                   double &acc1, double *tiles, int64_t *first_nz = nullptr) {
     const int lane = threadIdx.x & 31;
     double reg[kRows];
+    int64_t nz = n;  // kSumAndEnergy: this lane's first index whose x*x is nonzero
     auto load = [&](int64_t base) {
 #pragma unroll
         for (int r = 0; r < kRows; ++r) {
@@ -65,7 +66,10 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
             double t0, t1 = 0.0;
             tile_terms<KIND>(reg[r], base + r * 32 + lane, mean, t0, t1);
             c0[r * 32 + lane] = t0;
-            if (KIND == kSumAndEnergy) c1[r * 32 + lane] = t1;
+            if (KIND == kSumAndEnergy) {
+                c1[r * 32 + lane] = t1;
+                if (t1 != 0.0 && base + r * 32 + lane < nz) nz = base + r * 32 + lane;
+            }
         }
     };
     if (n <= 0) return;
@@ -103,6 +107,13 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
         __syncwarp();
         buf ^= 1;
     }
+    if (KIND == kSumAndEnergy && first_nz) {
+        for (int off = 16; off > 0; off >>= 1) {
+            const int64_t o = __shfl_down_sync(0xffffffffu, nz, off);
+            nz = o < nz ? o : nz;
+        }
+        *first_nz = nz;  // lane 0's value is the warp's
+    }
 }
 
 template <int KIND>
@@ -115,11 +126,13 @@ __global__ void __launch_bounds__(32 * kSerialWarps) serial_sum_kernel(const Sum
     const int64_t len = job.sig.len;
     const double mean = KIND == kNyquist ? job.out[0] / (double)len : 0.0;
     double acc0 = 0.0, acc1 = 0.0;
-    warp_serial<KIND>(job.sig, 0, len, mean, acc0, acc1, tiles[threadIdx.x >> 5]);
+    int64_t first_nz = len;
+    warp_serial<KIND>(job.sig, 0, len, mean, acc0, acc1, tiles[threadIdx.x >> 5], &first_nz);
     if (lane == 0) {
         if (KIND == kSumAndEnergy) {
             job.out[0] = acc0;
             job.out[2] = acc1;
+            job.out[3] = (double)first_nz;  // first index with a nonzero energy term (len if none)
         } else if (KIND == kNyquist) {
             job.out[1] = acc0;
         } else {
@@ -137,6 +150,9 @@ struct AlignedEnergyArgs {
     int64_t ref_len;
     const int64_t *lag;
     double *out;  // [energy, aligned length]
+    // the serial sums of the whole degraded signal ([sum, -, energy, first
+    // index with a nonzero energy term]), or null
+    const double *deg_stats;
 };
 
 __global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs,
@@ -158,6 +174,18 @@ __global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const
         } else {
             alen = L + lag;
         }
+    }
+    // The serial sum over samples skip.. equals the whole signal's when every
+    // dropped term is zero: the whole-signal chain holds +0 through them (a
+    // +0 term leaves +0 unchanged) and then adds the same terms in the same
+    // order. Delays, whose dropped samples are the prepended silence, take
+    // this path.
+    if (job.deg_stats && (double)skip <= job.deg_stats[3]) {
+        if (lane == 0) {
+            job.out[0] = job.deg_stats[2];
+            job.out[1] = (double)alen;
+        }
+        return;
     }
     double acc = 0.0, unused = 0.0;
     warp_serial<kEnergy>(job.deg, skip, L - skip, 0.0, acc, unused, tiles[threadIdx.x >> 5]);
@@ -409,8 +437,9 @@ void launch_aligned_energy_tree(const void *d_args, int njobs, double *d_scratch
 
 size_t aligned_energy_args_size() { return sizeof(AlignedEnergyArgs); }
 
-void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out) {
-    AlignedEnergyArgs a{deg, ref_len, d_lag, d_out};
+void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out,
+                              const double *d_deg_stats) {
+    AlignedEnergyArgs a{deg, ref_len, d_lag, d_out, d_deg_stats};
     *static_cast<AlignedEnergyArgs *>(dst) = a;
 }
 

@@ -57,13 +57,18 @@ struct FastBandCoeffs {
     double post64;             // |s1n0 a0^3|, applied to the RMS
     float beta[2];             // f32 form: numerators of stages 3-4
     float p1h, p1l, p2h, p2l;  // f32 form: poles d1, d2 as hi + lo f32 pairs
-    int32_t direct_i;          // f32 form: 1 direct form I, 0 transposed direct form II
+    int32_t arith;             // f32 form, per band group: kArith* below
 };
+
+// Arithmetic of a band group in the f32 form's gammatone kernel.
+constexpr int32_t kArithF32Df2t = 0;  // stages 3-4 f32, transposed direct form II
+constexpr int32_t kArithF32Df1 = 1;   // stages 3-4 f32, direct form I
+constexpr int32_t kArithF64 = 2;      // all four stages f64 (poles nearest the unit circle)
 
 // Arithmetic forms of the batch pipeline.
 enum Form : int32_t {
     kFormExact = 0,  // f64, no FMA, the CPU's operation order (bit-identical stages)
-    kFormF32 = 1,    // gammatone stages 2-4 in f32 (stage 1 f64), tree-summed statistics
+    kFormF32 = 1,    // gammatone stages 3-4 in f32 but in the lowest band group, tree-summed statistics
     kFormF64 = 2,    // gammatone in f64 with FMA (direct form I), tree-summed statistics
 };
 
@@ -74,7 +79,11 @@ uint64_t &launch_counter();
 void launch_envelope_stats(const SumJob *d_jobs, int njobs, cudaStream_t s);
 void launch_energy(const SumJob *d_jobs, int njobs, cudaStream_t s);
 size_t aligned_energy_args_size();
-void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out);
+// d_deg_stats: the exact form's serial sums of the whole degraded signal
+// (launch_envelope_stats), from which the aligned energy is taken when the
+// lag drops only zero terms; or null.
+void fill_aligned_energy_args(void *dst, const VSig &deg, int64_t ref_len, const int64_t *d_lag, double *d_out,
+                              const double *d_deg_stats = nullptr);
 void launch_aligned_energy(const void *d_args, int njobs, cudaStream_t s);
 void launch_pack(const LagJob *d_jobs, int njobs, int64_t max_n, bool raw, cudaStream_t s);
 size_t scale_args_size();
@@ -117,6 +126,23 @@ bool fused_lag_register_columns(int64_t n);
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
                       const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
                       cudaStream_t s);
+
+// k_lag.cu: the FP32 form's search (fused_lag_supported(n)): the same three
+// passes in f32, candidates within the f32 error bound of the maximum, f64
+// rescoring. Per job: z32 (n points), energy (lag32_parts(n)), cands
+// (lag32_parts(n)), status, ncand, cand_key (kLagCandCap), rescore
+// (kLagCandCap x nchunks, nchunks = lag32_rescore_chunks(the jobs' largest
+// b.len)). A job whose status is 1 afterwards has no lag: the caller reruns
+// it with launch_fused_lag. Twiddles: the f64 tables rounded to f32.
+void lag32_init_attributes();
+size_t lag32_parts(int64_t n);
+int lag32_rescore_chunks(int64_t max_b_len);
+void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const float2 *tcol, const float2 *tw_block,
+                  const float2 *tst, int nchunks, cudaStream_t s);
+// The nomination, pick and rescoring kernels on one job's caller-supplied
+// approximate correlation (corr_out, n values) with slack_fixed as the slack,
+// raw signals; the job's cands array holds ceil(n / 4096) records.
+void launch_refine_approx(const LagJob *d_job, int64_t n, int nchunks, cudaStream_t s);
 
 // k_gammatone.cu
 int gammatone_frames_per_cta(int nb);
@@ -172,6 +198,9 @@ int table_offsets_per_cta();
 std::vector<int> table_width_candidates(int P);
 void launch_table(const TableTask *d_tasks, int ntasks, int nb, int P, bool fast, int width, cudaStream_t s);
 void launch_stats(const StatsJob *d_jobs, int njobs, int nb, cudaStream_t s);
+// The fast forms' NSIM quotient n / d (d > 0, normal) elementwise, for its
+// direct test.
+void launch_fast_quotient(const double *num, const double *den, double *out, size_t count, cudaStream_t s);
 
 // k_dp.cu
 void launch_dp(const DpJob *d_jobs, int njobs, cudaStream_t s);

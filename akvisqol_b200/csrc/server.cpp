@@ -6,13 +6,20 @@
 // arena) and a host thread. A lane that is free takes the oldest queued
 // request, then every further queued request of the same mode and sample
 // rate, oldest first, while the batch stays within max_batch pairs and the
-// lane's share of the HBM budget (pair footprints are estimated from the
-// signal lengths), and runs the batch through its engine. A lane that
-// finishes goes straight back to the queue, so requests that arrived while
-// others were on the GPU are admitted as soon as a lane and its memory free
-// up, and up to `lanes` batches overlap on the device. Under light load
-// batches are small (low latency); under heavy load they grow to max_batch
-// (high throughput).
+// HBM the other lanes leave free, and runs the batch through its engine. A
+// lane that finishes goes straight back to the queue, so requests that
+// arrived while others were on the GPU are admitted as soon as a lane and
+// memory free up, and up to `lanes` batches overlap on the device. Under
+// light load batches are small (low latency); under heavy load they grow to
+// max_batch (high throughput).
+//
+// HBM is one pool: the budget is shared by all lanes, each counting what its
+// engines hold (their arenas grow to the largest batch they ran and are
+// reused) or, while it runs a batch, the larger of that and the batch's
+// footprint (pair footprints are upper bounds estimated from the signal
+// lengths). A request larger than what the other lanes leave makes idle
+// lanes give their memory back, then waits for the busy ones; only a pair
+// larger than the whole budget is refused.
 //
 // The pipeline's results for a pair do not depend on the other pairs of its
 // batch (each kernel job reads and writes only its own pair's buffers), so a
@@ -75,7 +82,7 @@ struct visqol_b200_server {
     vqb::Options opt[2];  // audio, speech
     std::shared_ptr<const vqb::host::Svr> svr;
     std::shared_ptr<const vqb::host::LatticeMapper> lattice;  // speech requests, when enabled
-    uint64_t budget = 0, lane_budget = 0;
+    uint64_t budget = 0;
     uint32_t max_batch = 64;
 
     std::mutex mu;
@@ -86,13 +93,24 @@ struct visqol_b200_server {
     uint64_t next_ticket = 1;
     uint64_t submitted = 0, completed = 0, failed = 0, in_flight = 0, in_flight_bytes = 0, batches = 0,
              batch_pairs = 0;
+    uint64_t gen = 0;  // bumped (under mu) when the queue or a lane's memory changes
     std::vector<double> latency, queueing;
 
     struct Lane {
         std::unique_ptr<vqb::Engine> engine[2];
         std::thread thread;
         uint64_t reserved = 0;  // device memory its engines hold (under mu)
+        uint64_t inflight = 0;  // footprint of the batch it runs (under mu)
+        bool busy = false;
     };
+
+    // HBM of the budget that the lanes other than `self` leave (under mu).
+    uint64_t pool_available(const Lane &self) const {
+        uint64_t held = 0;
+        for (auto &l : lanes)
+            if (l.get() != &self) held += l->busy ? std::max(l->reserved, l->inflight) : l->reserved;
+        return budget > held ? budget - held : 0;
+    }
     std::vector<std::unique_ptr<Lane>> lanes;
 
     // Stops the lanes (each finishes its batch in flight and what is still
@@ -120,36 +138,78 @@ struct visqol_b200_server {
         cudaSetDevice(device);
         for (;;) {
             std::vector<std::unique_ptr<Request>> batch;
+            bool release = false;
             {
                 std::unique_lock<std::mutex> lock(mu);
-                cv_work.wait(lock, [&] { return stopping || !queue.empty(); });
-                if (queue.empty()) return;  // stopping and drained
-                const uint32_t mode = queue.front()->mode, sr = queue.front()->sample_rate;
-                const bool dev = queue.front()->device;
-                uint64_t bytes = 0;
-                for (auto it = queue.begin(); it != queue.end() && batch.size() < max_batch;) {
-                    Request &r = **it;
-                    if (r.mode == mode && r.sample_rate == sr && r.device == dev &&
-                        (batch.empty() || bytes + r.footprint <= lane_budget)) {
-                        bytes += r.footprint;
-                        batch.push_back(std::move(*it));
-                        it = queue.erase(it);
-                    } else {
-                        ++it;
+                for (;;) {
+                    if (queue.empty()) {
+                        if (stopping) return;  // stopping and drained
+                        const uint64_t g = gen;
+                        cv_work.wait(lock, [&] { return stopping || gen != g; });
+                        continue;
                     }
+                    const uint64_t avail = pool_available(lane);
+                    if (queue.front()->footprint <= avail) {
+                        admit(lane, avail, batch);
+                        break;
+                    }
+                    // The oldest request does not fit beside what the other
+                    // lanes hold: hand this idle lane's memory back, or wait
+                    // for another lane to finish or to hand its memory back
+                    // (idle lanes holding memory are woken to do so).
+                    if (lane.reserved > 0) {
+                        release = true;
+                        break;
+                    }
+                    const uint64_t g = gen;
+                    cv_work.notify_all();
+                    cv_work.wait(lock, [&] { return gen != g; });
                 }
-                const auto now = Clock::now();
-                for (auto &r : batch) {
-                    r->admitted = now;
-                    queueing.push_back(ms_between(r->submitted, now));
+            }
+            if (release) {
+                for (auto &e : lane.engine)
+                    if (e) e->release_device_memory();
+                {
+                    std::lock_guard<std::mutex> lock(mu);
+                    lane.reserved = 0;
+                    ++gen;
                 }
-                in_flight += batch.size();
-                in_flight_bytes += bytes;
-                ++batches;
-                batch_pairs += batch.size();
+                cv_work.notify_all();
+                continue;
             }
             run(lane, batch);
         }
+    }
+
+    // The oldest request and every further queued one of its mode, sample
+    // rate and input kind, oldest first, within max_batch pairs and `avail`
+    // bytes (under mu; the oldest fits).
+    void admit(Lane &lane, uint64_t avail, std::vector<std::unique_ptr<Request>> &batch) {
+        const uint32_t mode = queue.front()->mode, sr = queue.front()->sample_rate;
+        const bool dev = queue.front()->device;
+        uint64_t bytes = 0;
+        for (auto it = queue.begin(); it != queue.end() && batch.size() < max_batch;) {
+            Request &r = **it;
+            if (r.mode == mode && r.sample_rate == sr && r.device == dev && bytes + r.footprint <= avail) {
+                bytes += r.footprint;
+                batch.push_back(std::move(*it));
+                it = queue.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        const auto now = Clock::now();
+        for (auto &r : batch) {
+            r->admitted = now;
+            queueing.push_back(ms_between(r->submitted, now));
+        }
+        lane.busy = true;
+        lane.inflight = bytes;
+        in_flight += batch.size();
+        in_flight_bytes += bytes;
+        ++batches;
+        batch_pairs += batch.size();
+        ++gen;
     }
 
     void run(Lane &lane, std::vector<std::unique_ptr<Request>> &batch) {
@@ -210,8 +270,12 @@ struct visqol_b200_server {
             lane.reserved = 0;
             for (auto &e : lane.engine)
                 if (e) lane.reserved += e->reserved_bytes();
+            lane.busy = false;
+            lane.inflight = 0;
+            ++gen;
         }
         cv_done.notify_all();
+        cv_work.notify_all();
     }
 };
 
@@ -258,7 +322,6 @@ int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serv
         if (s->budget > free_b) return fail(VISQOL_E_OUT_OF_MEMORY, "hbm_budget_bytes exceeds the free device memory");
         const uint32_t lanes = c.lanes ? std::min<uint32_t>(c.lanes, 16) : 4;
         s->max_batch = c.max_batch ? c.max_batch : 64;
-        s->lane_budget = s->budget / lanes;
         for (uint32_t l = 0; l < lanes; ++l) s->lanes.push_back(std::make_unique<visqol_b200_server::Lane>());
         visqol_b200_server *raw = s.get();
         for (auto &l : s->lanes) {
@@ -278,6 +341,14 @@ int visqol_b200_server_create(const visqol_options *opts, const visqol_b200_serv
 
 void visqol_b200_server_destroy(visqol_b200_server *s) { delete s; }
 
+int visqol_b200_pair_footprint(size_t ref_len, size_t deg_len, uint32_t sample_rate, uint32_t mode,
+                               uint64_t *bytes) {
+    if (!bytes || sample_rate == 0 || mode > VISQOL_MODE_SPEECH)
+        return fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    *bytes = vqb::Engine::pair_footprint(ref_len, deg_len, sample_rate, mode == VISQOL_MODE_SPEECH);
+    return VISQOL_OK;
+}
+
 int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double *ref, size_t ref_len,
                               const double *deg, size_t deg_len, uint32_t sample_rate, uint32_t flags,
                               uint64_t *ticket) {
@@ -293,8 +364,8 @@ int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double
     r->deg_len = deg_len;
     try {
         r->footprint = vqb::Engine::pair_footprint(ref_len, deg_len, sample_rate, mode == VISQOL_MODE_SPEECH);
-        if (r->footprint > s->lane_budget)
-            return fail(VISQOL_E_OUT_OF_MEMORY, "pair exceeds one lane's share of the HBM budget");
+        if (r->footprint > s->budget)
+            return fail(VISQOL_E_OUT_OF_MEMORY, "pair exceeds the server's HBM budget");
         if (r->device) {
             r->ref_ptr = ref;
             r->deg_ptr = deg;
@@ -315,8 +386,9 @@ int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double
         if (s->stopping) return fail(VISQOL_E_INVALID_ARGUMENT, "server is stopping");
         ++s->submitted;
         s->queue.push_back(std::move(r));
+        ++s->gen;
     }
-    s->cv_work.notify_one();
+    s->cv_work.notify_all();
     return VISQOL_OK;
 }
 

@@ -2,6 +2,7 @@
 // buffers in, runs one kernel family of the batch pipeline, and copies the
 // result out. They exist so that each kernel can be checked on its own
 // against the CPU model; the batch pipeline does not use them.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -41,17 +42,20 @@ struct DBuf {
     }
 };
 
-// One engine per process for the stage calls (its stream and caches).
-vqb::Engine &stage_engine() {
+// One engine per process and arithmetic form for the stage calls (its
+// stream and caches).
+vqb::Engine &stage_engine(int form = vqb::kFormExact) {
     static std::mutex mu;
-    static std::unique_ptr<vqb::Engine> e;
+    static std::unique_ptr<vqb::Engine> e[3];
     std::lock_guard<std::mutex> lock(mu);
-    if (!e) {
+    if (!e[form]) {
         int dev = 0;
         cudaGetDevice(&dev);
-        e = std::make_unique<vqb::Engine>(dev, vqb::Options{}, nullptr);
+        vqb::Options o;
+        o.form = form;
+        e[form] = std::make_unique<vqb::Engine>(dev, o, nullptr);
     }
-    return *e;
+    return *e[form];
 }
 
 template <class F>
@@ -106,6 +110,54 @@ int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t
 
 int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb, int64_t *lag) {
     return lag_stage(a, la, b, lb, lag, true);
+}
+
+int visqol_b200_lag_search(const double *a, size_t la, const double *b, size_t lb, int raw, int form, int64_t *lag,
+                           int32_t *undecided, float *corr, size_t corr_len) {
+    if ((!a && la) || (!b && lb) || !lag || (form != 0 && form != 1))
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    const size_t n = vqb::host::fft_size_for(std::max(la, lb));
+    if (corr && (form != 1 || corr_len != n || std::max(la, lb) == 0 || n > ((size_t)1 << 24)))
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "corr needs form 1 and corr_len = fftSizeFor(max(la, lb))");
+    return guarded([&] {
+        DBuf<double> da(a, la), db(b, lb);
+        std::unique_ptr<DBuf<float>> dc;
+        if (corr) dc = std::make_unique<DBuf<float>>(n);
+        const vqb::VSig va{da.p, 0, (int64_t)la, (int64_t)la}, vb{db.p, 0, (int64_t)lb, (int64_t)lb};
+        int32_t st = 0;
+        stage_engine(form == 1 ? vqb::kFormF32 : vqb::kFormExact)
+            .lags(1, &va, &vb, raw != 0, lag, &st, dc ? dc->p : nullptr);
+        if (undecided) *undecided = st;
+        if (dc) dc->get(corr, n);
+    });
+}
+
+int visqol_b200_refine_lag(const double *s1, size_t l1, const double *s2, size_t l2, const float *approx, size_t n,
+                           double scale, double tol, int64_t *lag, int32_t *decided) {
+    if ((!s1 && l1) || (!s2 && l2) || !approx || !lag || !decided || l1 == 0 || l2 == 0 ||
+        n < 2 * std::max(l1, l2) - 1 || n > ((size_t)1 << 31))
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument (n must be at least 2 max(l1, l2) - 1)");
+    return guarded([&] {
+        double e1 = 0.0, e2 = 0.0;
+        for (size_t i = 0; i < l1; ++i) e1 += s1[i] * s1[i];
+        for (size_t i = 0; i < l2; ++i) e2 += s2[i] * s2[i];
+        const double slack = 2.0 * tol * (e1 + e2) * scale;
+        DBuf<double> da(s1, l1), db(s2, l2);
+        DBuf<float> dx(approx, n);
+        const vqb::VSig va{da.p, 0, (int64_t)l1, (int64_t)l1}, vb{db.p, 0, (int64_t)l2, (int64_t)l2};
+        *decided = stage_engine(vqb::kFormF32).refine_approx(va, vb, dx.p, (int64_t)n, slack, lag) ? 1 : 0;
+    });
+}
+
+int visqol_b200_nsim_quotient(const double *num, const double *den, size_t n, double *out) {
+    if ((!num || !den || !out) && n) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        vqb::Engine &e = stage_engine();
+        DBuf<double> dn(num, n), dd(den, n), dq(n);
+        vqb::launch_fast_quotient(dn.p, dd.p, dq.p, n, e.stream());
+        VQB_CUDA(cudaStreamSynchronize(e.stream()));
+        dq.get(out, n);
+    });
 }
 
 int visqol_b200_fft(double *buf, size_t n, int inverse) {

@@ -1,12 +1,13 @@
 """ctypes binding of libvisqol (include/visqol.h + include/visqol_b200.h).
 
-Mirrors the reference's Python binding (src/python/visqol/_native.py:32-248):
-the same ``Options``/``Patch``/``Result`` structures, ``Context`` with
-``measure``/``measure_batch``/``measure_files``/``measure_files_batch``,
-``NativeError`` carrying the C error code, and ``free``/``vec`` helpers, so
-code written against that module reads the same here. Extensions: traced
-batches (per-pair lags and matches), device-resident inputs, per-stage
-timing, and single-stage calls.
+The ABI's structures (``Options``, ``Patch``, ``Result``; their layouts are
+fixed by include/visqol.h, as in the reference's src/include/visqol.h) and a
+``Context`` over one ``visqol_ctx`` with scoring of pairs, batches and WAV
+files, plus this library's extensions: traced batches (per-pair lags and
+matches), device-resident inputs, prepared references, the request server,
+per-stage timing, and single-stage calls. The reference's own Python
+package binds the same ABI with its own module and loads this library
+unchanged.
 
 There is no fallback: if ``libvisqol.so`` is missing, importing this module
 raises ImportError.
@@ -17,7 +18,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
-from ctypes import (POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_size_t, c_uint8, c_uint32,
+from ctypes import (POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint8, c_uint32,
                     c_uint64, c_void_p)
 from pathlib import Path
 
@@ -87,6 +88,7 @@ class Timing(ctypes.Structure):
         ("nsim_ms", c_double), ("realign_ms", c_double), ("gammatone_kernel_ms", c_double),
         ("gammatone_launches", c_uint64), ("gammatone_rms", c_uint64), ("gammatone_window", c_uint64),
         ("kernel_launches", c_uint64), ("h2d_bytes", c_uint64), ("d2h_bytes", c_uint64), ("host_syncs", c_uint64),
+        ("lag_kernel_ms", c_double), ("lag_bytes", c_uint64), ("lag_reruns", c_uint64),
     ]
 
 
@@ -127,8 +129,8 @@ def _load() -> ctypes.CDLL:
         "visqol_destroy": (None, [c_void_p]),
         "visqol_measure": (c_int, [c_void_p, D, c_size_t, D, c_size_t, c_uint32, POINTER(POINTER(Result))]),
         "visqol_measure_files": (c_int, [c_void_p, c_char_p, c_char_p, POINTER(POINTER(Result))]),
-        "visqol_measure_batch": (c_int, [c_void_p, c_size_t, POINTER(D), SZ, POINTER(D), SZ, c_uint32, c_uint32,
-                                         POINTER(POINTER(Result)), POINTER(c_int32)]),
+        "visqol_measure_batch": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, POINTER(c_void_p), SZ, c_uint32,
+                                         c_uint32, POINTER(POINTER(Result)), POINTER(c_int32)]),
         "visqol_measure_files_batch": (c_int, [c_void_p, c_size_t, POINTER(c_char_p), POINTER(c_char_p), c_uint32,
                                                POINTER(POINTER(Result)), POINTER(c_int32)]),
         "visqol_result_free": (None, [POINTER(Result)]),
@@ -142,7 +144,12 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_spectrogram": (c_int, [c_size_t, D, D, c_size_t, c_size_t, D, c_size_t, D, SZ]),
         "visqol_b200_envelope_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
         "visqol_b200_best_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
+        "visqol_b200_lag_search": (c_int, [D, c_size_t, D, c_size_t, c_int, c_int, I64, POINTER(c_int32),
+                                           POINTER(c_float), c_size_t]),
+        "visqol_b200_refine_lag": (c_int, [D, c_size_t, D, c_size_t, POINTER(c_float), c_size_t, c_double, c_double,
+                                           I64, POINTER(c_int32)]),
         "visqol_b200_fft": (c_int, [D, c_size_t, c_int]),
+        "visqol_b200_nsim_quotient": (c_int, [D, D, c_size_t, D]),
         "visqol_b200_prepare_for_comparison": (c_int, [D, D, c_size_t, c_size_t, c_size_t]),
         "visqol_b200_log10": (c_int, [D, c_size_t, D]),
         "visqol_b200_nsim_table": (c_int, [D, c_size_t, D, c_size_t, c_size_t, c_size_t, c_size_t, I64, I64, I64, D]),
@@ -164,6 +171,7 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_server_next": (c_int, [c_void_p, c_int32, POINTER(c_uint64), POINTER(c_int32),
                                             POINTER(POINTER(Result))]),
         "visqol_b200_server_stats": (c_int, [c_void_p, POINTER(ServeStats), c_int]),
+        "visqol_b200_pair_footprint": (c_int, [c_size_t, c_size_t, c_uint32, c_uint32, POINTER(c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -187,44 +195,57 @@ EXPORTS = [
     "visqol_measure_batch", "visqol_measure_files_batch", "visqol_result_free",
     "visqol_b200_measure_batch", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
     "visqol_b200_spectrogram", "visqol_b200_envelope_lag", "visqol_b200_best_lag", "visqol_b200_fft",
+    "visqol_b200_lag_search", "visqol_b200_refine_lag", "visqol_b200_nsim_quotient",
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
     "visqol_b200_lattice_predict", "visqol_b200_autotune_choices",
     "visqol_b200_prepare", "visqol_b200_measure_prepared", "visqol_b200_prepared_free",
     "visqol_b200_server_create", "visqol_b200_server_destroy", "visqol_b200_server_submit",
-    "visqol_b200_server_next", "visqol_b200_server_stats",
+    "visqol_b200_server_next", "visqol_b200_server_stats", "visqol_b200_pair_footprint",
 ]
 
 
+# Status names of include/visqol.h, for messages.
+_STATUS = {OK: "OK", E_INVALID_ARGUMENT: "INVALID_ARGUMENT", E_OUT_OF_MEMORY: "OUT_OF_MEMORY", E_IO: "IO",
+           E_MODEL: "MODEL", E_SIGNAL: "SIGNAL", E_BACKEND: "BACKEND", E_INTERNAL: "INTERNAL"}
+
+
 class NativeError(RuntimeError):
+    """A non-zero status from libvisqol: ``code`` is the negative status of
+    include/visqol.h; the message is the library's text for the failure."""
+
     def __init__(self, code: int, message: str):
-        super().__init__(message)
-        self.code = code
+        self.code = int(code)
+        super().__init__(f"{_STATUS.get(self.code, self.code)}: {message}")
 
 
-def last_error(code: int) -> NativeError:
-    return NativeError(code, (lib.visqol_last_error() or b"").decode(errors="replace"))
+def error_for(code: int) -> NativeError:
+    """`code` with the calling thread's last library message."""
+    text = lib.visqol_last_error()
+    return NativeError(code, text.decode("utf-8", "replace") if text else "")
 
 
 def _check(rc: int) -> None:
-    if rc != OK:
-        raise last_error(rc)
+    if rc:
+        raise error_for(rc)
 
 
 def available_backends() -> list[str]:
-    mask = lib.visqol_available_backends()
-    return [name for name, bit in BACKENDS.items() if mask & (1 << bit)]
+    """Backends this library runs, by name (its bit mask)."""
+    mask = int(lib.visqol_available_backends())
+    return [b for b, bit in sorted(BACKENDS.items(), key=lambda kv: kv[1]) if mask >> bit & 1]
 
 
-def as_signal(x, name: str) -> np.ndarray:
-    a = np.ascontiguousarray(x, dtype=np.float64)
-    if a.ndim != 1:
-        raise ValueError(f"{name} must be a 1-D mono signal, got shape {a.shape}")
-    return a
+def mono(x, what: str = "signal") -> np.ndarray:
+    """x as contiguous float64 samples; copies only when it must."""
+    arr = np.ascontiguousarray(x, dtype=np.float64)
+    if arr.ndim != 1:
+        raise ValueError(f"{what}: mono samples expected (a 1-D array), not shape {arr.shape}")
+    return arr
 
 
-def _ptr(a: np.ndarray):
+def _dptr(a: np.ndarray):
     return a.ctypes.data_as(POINTER(c_double))
 
 
@@ -232,44 +253,98 @@ def _i64(a: np.ndarray):
     return a.ctypes.data_as(POINTER(c_int64))
 
 
+class _Signals:
+    """A batch's signal table as the C calls take it: an array of sample
+    pointers and one of lengths. Host signals are converted to float64 and
+    held here for the call's lifetime; device signals are addresses (ints)
+    with their lengths."""
+
+    def __init__(self, signals, lengths=None, device: bool = False):
+        n = len(signals)
+        if device:
+            if lengths is None or len(lengths) != n:
+                raise ValueError("device signals need one length each")
+            self.hold = ()
+            addrs, counts = [int(p) for p in signals], [int(c) for c in lengths]
+        else:
+            self.hold = [mono(x) for x in signals]
+            addrs, counts = [a.ctypes.data for a in self.hold], [a.size for a in self.hold]
+        self.ptrs = (c_void_p * n)(*addrs)
+        self.lens = (c_size_t * n)(*counts)
+
+
+def _outcomes(outs, status, n: int) -> list:
+    """Per pair: its Result pointer, or a NativeError with its status."""
+    got = []
+    for i in range(n):
+        code = int(status[i])
+        got.append(outs[i] if code == OK else NativeError(code, f"pair {i} failed"))
+    return got
+
+
+# Context keyword -> (Options field, conversion)
+_OPTION_FIELDS = {
+    "mode": ("mode", int),
+    "search_window_radius": ("search_window_radius", int),
+    "use_unscaled_speech_mos_mapping": ("use_unscaled_speech_mos_mapping", lambda v: int(bool(v))),
+    "disable_global_alignment": ("disable_global_alignment", lambda v: int(bool(v))),
+    "disable_realignment": ("disable_realignment", lambda v: int(bool(v))),
+    "use_lattice_model": ("use_lattice_model", lambda v: int(bool(v))),
+}
+
+
+def make_options(backend: str = "cuda", precision: str | None = None, model_path: str | None = None,
+                 **settings) -> Options:
+    """visqol_options from the library defaults, overridden by keyword."""
+    if backend not in BACKENDS:
+        raise ValueError(f"backend {backend!r} is none of {', '.join(sorted(BACKENDS))}")
+    if precision is not None and precision not in PRECISIONS:
+        raise ValueError(f"precision {precision!r} is none of {', '.join(sorted(PRECISIONS))}")
+    opts = Options()
+    lib.visqol_options_default(ctypes.byref(opts))
+    for key, value in settings.items():
+        if key not in _OPTION_FIELDS:
+            raise TypeError(f"unknown option {key!r}")
+        field, conv = _OPTION_FIELDS[key]
+        setattr(opts, field, conv(value))
+    opts.model_path = os.fsencode(model_path) if model_path else None
+    opts.backend = BACKENDS[backend]
+    if precision is not None:
+        opts.precision = PRECISIONS[precision]
+    return opts
+
+
 class Context:
-    """Owns a ``visqol_ctx`` (one thread at a time)."""
+    """A ``visqol_ctx``: options fixed at creation, one thread at a time.
+
+    Scoring calls return ``Result`` pointers (free them with ``free``), and
+    batch calls a list with a ``NativeError`` in place of each failed pair.
+    """
 
     def __init__(self, *, mode: int = MODE_AUDIO, search_window_radius: int = 60,
                  use_unscaled_speech_mos_mapping: bool = False, disable_global_alignment: bool = False,
                  disable_realignment: bool = False, use_lattice_model: bool = False, model_path: str | None = None,
                  backend: str = "cuda", precision: str | None = None):
-        if backend not in BACKENDS:
-            raise ValueError(f"unknown backend {backend!r}; expected one of {sorted(BACKENDS)}")
-        if precision is not None and precision not in PRECISIONS:
-            raise ValueError(f"unknown precision {precision!r}; expected one of {sorted(PRECISIONS)}")
-        opts = Options()
-        lib.visqol_options_default(ctypes.byref(opts))
-        opts.mode = mode
-        opts.search_window_radius = search_window_radius
-        opts.use_unscaled_speech_mos_mapping = int(bool(use_unscaled_speech_mos_mapping))
-        opts.disable_global_alignment = int(bool(disable_global_alignment))
-        opts.disable_realignment = int(bool(disable_realignment))
-        opts.use_lattice_model = int(bool(use_lattice_model))
-        opts.model_path = os.fsencode(model_path) if model_path else None
-        opts.backend = BACKENDS[backend]
-        if precision is not None:
-            opts.precision = PRECISIONS[precision]
+        opts = make_options(backend, precision, model_path, mode=mode, search_window_radius=search_window_radius,
+                            use_unscaled_speech_mos_mapping=use_unscaled_speech_mos_mapping,
+                            disable_global_alignment=disable_global_alignment,
+                            disable_realignment=disable_realignment, use_lattice_model=use_lattice_model)
         handle = c_void_p()
         _check(lib.visqol_create(ctypes.byref(opts), ctypes.byref(handle)))
         self._handle = handle
 
     def close(self) -> None:
-        if getattr(self, "_handle", None):
-            lib.visqol_destroy(self._handle)
-            self._handle = None
+        handle, self._handle = getattr(self, "_handle", None), None
+        if handle:
+            lib.visqol_destroy(handle)
 
     def __del__(self):
         self.close()
 
-    def measure(self, ref: np.ndarray, deg: np.ndarray, sample_rate: int):
+    def measure(self, ref, deg, sample_rate: int):
+        ref, deg = mono(ref, "ref"), mono(deg, "deg")
         out = POINTER(Result)()
-        _check(lib.visqol_measure(self._handle, _ptr(ref), ref.size, _ptr(deg), deg.size, sample_rate,
+        _check(lib.visqol_measure(self._handle, _dptr(ref), ref.size, _dptr(deg), deg.size, sample_rate,
                                   ctypes.byref(out)))
         return out
 
@@ -279,17 +354,22 @@ class Context:
                                         ctypes.byref(out)))
         return out
 
-    def measure_batch(self, refs: list[np.ndarray], degs: list[np.ndarray], sample_rate: int, num_threads: int = 0):
-        n = len(refs)
-        ref_ptrs = (POINTER(c_double) * n)(*[_ptr(a) for a in refs])
-        deg_ptrs = (POINTER(c_double) * n)(*[_ptr(a) for a in degs])
-        ref_lens = (c_size_t * n)(*[a.size for a in refs])
-        deg_lens = (c_size_t * n)(*[a.size for a in degs])
-        outs = (POINTER(Result) * n)()
-        status = (c_int32 * n)()
-        lib.visqol_measure_batch(self._handle, n, ref_ptrs, ref_lens, deg_ptrs, deg_lens, sample_rate, num_threads,
-                                 outs, status)
-        return _collect(outs, status, n)
+    def _pairs_call(self, fn, n: int, *args):
+        outs, status = (POINTER(Result) * n)(), (c_int32 * n)()
+        rc = fn(self._handle, n, *args, outs, status)
+        if rc and all(int(status[i]) == OK for i in range(n)):
+            raise error_for(rc)  # the call itself was refused
+        return _outcomes(outs, status, n)
+
+    def measure_batch(self, refs, degs, sample_rate: int, num_threads: int = 0):
+        r, d = _Signals(refs), _Signals(degs)
+        return self._pairs_call(lib.visqol_measure_batch, len(refs), r.ptrs, r.lens, d.ptrs, d.lens, sample_rate,
+                                num_threads)
+
+    def measure_files_batch(self, ref_paths, deg_paths, num_threads: int = 0):
+        n = len(ref_paths)
+        enc = lambda paths: (c_char_p * n)(*map(os.fsencode, paths))  # noqa: E731
+        return self._pairs_call(lib.visqol_measure_files_batch, n, enc(ref_paths), enc(deg_paths), num_threads)
 
     def prepare(self, refs, sample_rate: int, device_inputs: bool = False, ref_lens=None) -> "Prepared":
         """Reference-side work for scoring many degraded signals against
@@ -298,92 +378,58 @@ class Context:
 
     def measure_prepared(self, prepared: "Prepared", degs, ref_index=None, device_inputs: bool = False,
                          deg_lens=None):
-        """degs[i] against prepared reference ref_index[i] (default i):
-        per-pair Result pointers or NativeError, as measure_batch."""
+        """degs[i] against prepared reference ref_index[i] (default i), as
+        measure_batch."""
         n = len(degs)
-        if device_inputs:
-            dp = (c_void_p * n)(*degs)
-            dl = (c_size_t * n)(*deg_lens)
-        else:
-            degs = [np.ascontiguousarray(d, dtype=np.float64) for d in degs]
-            dp = (c_void_p * n)(*[d.ctypes.data for d in degs])
-            dl = (c_size_t * n)(*[d.size for d in degs])
+        d = _Signals(degs, deg_lens, device_inputs)
         ix = (c_size_t * n)(*ref_index) if ref_index is not None else None
-        outs = (POINTER(Result) * n)()
-        status = (c_int32 * n)()
-        rc = lib.visqol_b200_measure_prepared(self._handle, prepared._handle, n, ix, dp, dl,
-                                              DEVICE_INPUTS if device_inputs else 0, outs, status)
-        if rc != OK and all(status[i] == OK for i in range(n)):
-            raise last_error(rc)  # the call itself was refused
-        return _collect(outs, status, n)
+        flags = DEVICE_INPUTS if device_inputs else 0
+        outs, status = (POINTER(Result) * n)(), (c_int32 * n)()
+        rc = lib.visqol_b200_measure_prepared(self._handle, prepared._handle, n, ix, d.ptrs, d.lens, flags, outs,
+                                              status)
+        if rc and all(int(status[i]) == OK for i in range(n)):
+            raise error_for(rc)
+        return _outcomes(outs, status, n)
 
-    def measure_files_batch(self, ref_paths: list[str], deg_paths: list[str], num_threads: int = 0):
-        n = len(ref_paths)
-        refs = (c_char_p * n)(*[os.fsencode(p) for p in ref_paths])
-        degs = (c_char_p * n)(*[os.fsencode(p) for p in deg_paths])
-        outs = (POINTER(Result) * n)()
-        status = (c_int32 * n)()
-        lib.visqol_measure_files_batch(self._handle, n, refs, degs, num_threads, outs, status)
-        return _collect(outs, status, n)
+    def _b200_batch(self, refs, degs, sample_rate, device_inputs, ref_lens, deg_lens, traces):
+        n = len(refs)
+        r = _Signals(refs, ref_lens, device_inputs)
+        d = _Signals(degs, deg_lens, device_inputs)
+        outs, status = (POINTER(Result) * n)(), (c_int32 * n)()
+        lib.visqol_b200_measure_batch(self._handle, n, r.ptrs, r.lens, d.ptrs, d.lens, sample_rate,
+                                      DEVICE_INPUTS if device_inputs else 0, outs, status, traces)
+        return outs, status
 
     def measure_batch_scores(self, refs, degs, sample_rate: int, device_inputs: bool = False,
                              ref_lens=None, deg_lens=None):
-        """Batch without traces: a list of ``(code, MOS or None)`` (the
+        """Batch without traces: ``(code, MOS or None)`` per pair (the
         results are freed here)."""
-        n = len(refs)
-        if device_inputs:
-            rp = (c_void_p * n)(*[int(a) for a in refs])
-            dp = (c_void_p * n)(*[int(a) for a in degs])
-            rl = (c_size_t * n)(*ref_lens)
-            dl = (c_size_t * n)(*deg_lens)
-        else:
-            rp = (c_void_p * n)(*[a.ctypes.data for a in refs])
-            dp = (c_void_p * n)(*[a.ctypes.data for a in degs])
-            rl = (c_size_t * n)(*[a.size for a in refs])
-            dl = (c_size_t * n)(*[a.size for a in degs])
-        outs = (POINTER(Result) * n)()
-        status = (c_int32 * n)()
-        lib.visqol_b200_measure_batch(self._handle, n, rp, rl, dp, dl, sample_rate,
-                                      DEVICE_INPUTS if device_inputs else 0, outs, status, None)
-        res = []
-        for i in range(n):
-            if status[i] == OK:
-                res.append((OK, outs[i].contents.moslqo))
+        outs, status = self._b200_batch(refs, degs, sample_rate, device_inputs, ref_lens, deg_lens, None)
+        scores = []
+        for i in range(len(refs)):
+            if int(status[i]) == OK:
+                scores.append((OK, outs[i].contents.moslqo))
                 free(outs[i])
             else:
-                res.append((status[i], None))
-        return res
+                scores.append((int(status[i]), None))
+        return scores
 
     def measure_batch_traced(self, refs, degs, sample_rate: int, device_inputs: bool = False,
                              ref_lens=None, deg_lens=None):
         """Batch with per-pair traces. Host arrays, or device addresses (ints)
         with their lengths when ``device_inputs``. Returns a list of
         ``(code, result dict or None, trace dict or None)``."""
-        n = len(refs)
-        if device_inputs:
-            rp = (c_void_p * n)(*[int(a) for a in refs])
-            dp = (c_void_p * n)(*[int(a) for a in degs])
-            rl = (c_size_t * n)(*ref_lens)
-            dl = (c_size_t * n)(*deg_lens)
-        else:
-            rp = (c_void_p * n)(*[a.ctypes.data for a in refs])
-            dp = (c_void_p * n)(*[a.ctypes.data for a in degs])
-            rl = (c_size_t * n)(*[a.size for a in refs])
-            dl = (c_size_t * n)(*[a.size for a in degs])
-        outs = (POINTER(Result) * n)()
-        traces = (POINTER(Trace) * n)()
-        status = (c_int32 * n)()
-        lib.visqol_b200_measure_batch(self._handle, n, rp, rl, dp, dl, sample_rate,
-                                      DEVICE_INPUTS if device_inputs else 0, outs, status, traces)
-        res = []
-        for i in range(n):
-            if status[i] == OK:
-                res.append((OK, result_dict(outs[i].contents), trace_dict(traces[i].contents)))
+        traces = (POINTER(Trace) * len(refs))()
+        outs, status = self._b200_batch(refs, degs, sample_rate, device_inputs, ref_lens, deg_lens, traces)
+        got = []
+        for i in range(len(refs)):
+            if int(status[i]) == OK:
+                got.append((OK, result_dict(outs[i].contents), trace_dict(traces[i].contents)))
                 free(outs[i])
                 lib.visqol_b200_trace_free(traces[i])
             else:
-                res.append((status[i], None, None))
-        return res
+                got.append((int(status[i]), None, None))
+        return got
 
     def last_timing(self) -> dict:
         t = Timing()
@@ -391,17 +437,13 @@ class Context:
         return {name: getattr(t, name) for name, _ in Timing._fields_}
 
 
-def _collect(outs, status, n: int) -> list:
-    """Per-pair ``Result`` pointers, or ``NativeError`` for failed pairs."""
-    return [outs[i] if status[i] == OK else NativeError(status[i], f"pair {i}: error code {status[i]}")
-            for i in range(n)]
-
-
 def free(result) -> None:
+    """Release a Result the library returned."""
     lib.visqol_result_free(result)
 
 
 def vec(ptr, n: int) -> np.ndarray:
+    """n doubles at ptr, copied."""
     return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0)
 
 
@@ -458,30 +500,70 @@ def peak_tflops(kind: int) -> float:
 # ---- single-stage calls (exact f64 kernels on host buffers) ----------------
 
 def spectrogram(x, coeffs: np.ndarray, hann: np.ndarray, window: int, hop: int) -> np.ndarray:
-    x = as_signal(x, "x")
+    x = mono(x, "x")
     c = np.ascontiguousarray(coeffs, dtype=np.float64).reshape(-1)
     h = np.ascontiguousarray(hann, dtype=np.float64)
     nb = c.size // 8
     nf_max = 0 if x.size < window else 1 + (x.size - window) // hop
     out = np.zeros(max(1, nb * nf_max))
     nf = c_size_t()
-    _check(lib.visqol_b200_spectrogram(nb, _ptr(c), _ptr(h), window, hop, _ptr(x), x.size, _ptr(out),
+    _check(lib.visqol_b200_spectrogram(nb, _dptr(c), _dptr(h), window, hop, _dptr(x), x.size, _dptr(out),
                                        ctypes.byref(nf)))
     return out[: nb * nf.value].reshape(nb, nf.value)
 
 
 def envelope_lag(a, b) -> int:
-    a, b = as_signal(a, "a"), as_signal(b, "b")
+    a, b = mono(a, "a"), mono(b, "b")
     lag = c_int64()
-    _check(lib.visqol_b200_envelope_lag(_ptr(a), a.size, _ptr(b), b.size, ctypes.byref(lag)))
+    _check(lib.visqol_b200_envelope_lag(_dptr(a), a.size, _dptr(b), b.size, ctypes.byref(lag)))
     return lag.value
 
 
 def best_lag(a, b) -> int:
-    a, b = as_signal(a, "a"), as_signal(b, "b")
+    a, b = mono(a, "a"), mono(b, "b")
     lag = c_int64()
-    _check(lib.visqol_b200_best_lag(_ptr(a), a.size, _ptr(b), b.size, ctypes.byref(lag)))
+    _check(lib.visqol_b200_best_lag(_dptr(a), a.size, _dptr(b), b.size, ctypes.byref(lag)))
     return lag.value
+
+
+def lag_search(a, b, raw: bool = False, form: str = "exact", corr: bool = False):
+    """One pair's lag by the exact search or the FP32 form's ("fast"):
+    (lag, undecided, f32 correlation or None); see visqol_b200_lag_search."""
+    a, b = mono(a, "a"), mono(b, "b")
+    lag, und = c_int64(), c_int32()
+    out, n = None, 0
+    if corr:
+        n = 1
+        while n < 2 * max(a.size, b.size) - 1:
+            n <<= 1
+        out = np.zeros(n, np.float32)
+    code = lib.visqol_b200_lag_search(_dptr(a), a.size, _dptr(b), b.size, int(raw), 1 if form == "fast" else 0,
+                                      ctypes.byref(lag), ctypes.byref(und),
+                                      out.ctypes.data_as(POINTER(c_float)) if corr else None, n)
+    _check(code)
+    return lag.value, und.value, out
+
+
+def refine_lag(s1, s2, approx, scale: float, tol: float):
+    """Device refineLag on a caller's approximate correlation: the lag, or
+    None where more than 64 lags qualify."""
+    s1, s2 = mono(s1, "s1"), mono(s2, "s2")
+    approx = np.ascontiguousarray(approx, dtype=np.float32)
+    lag, decided = c_int64(), c_int32()
+    _check(lib.visqol_b200_refine_lag(_dptr(s1), s1.size, _dptr(s2), s2.size,
+                                      approx.ctypes.data_as(POINTER(c_float)), approx.size, scale, tol,
+                                      ctypes.byref(lag), ctypes.byref(decided)))
+    return lag.value if decided.value else None
+
+
+def nsim_quotient(num, den) -> np.ndarray:
+    """The fast forms' NSIM quotient num / den elementwise on the device."""
+    num, den = mono(num, "num"), mono(den, "den")
+    if num.size != den.size:
+        raise ValueError("num and den differ in length")
+    out = np.empty(num.size)
+    _check(lib.visqol_b200_nsim_quotient(_dptr(num), _dptr(den), num.size, _dptr(out)))
+    return out
 
 
 def fft(z: np.ndarray, inverse: bool = False) -> np.ndarray:
@@ -493,14 +575,14 @@ def fft(z: np.ndarray, inverse: bool = False) -> np.ndarray:
 def prepare_for_comparison(ref: np.ndarray, deg: np.ndarray):
     r = np.ascontiguousarray(ref, dtype=np.float64).copy()
     d = np.ascontiguousarray(deg, dtype=np.float64).copy()
-    _check(lib.visqol_b200_prepare_for_comparison(_ptr(r), _ptr(d), r.shape[0], r.shape[1], d.shape[1]))
+    _check(lib.visqol_b200_prepare_for_comparison(_dptr(r), _dptr(d), r.shape[0], r.shape[1], d.shape[1]))
     return r, d
 
 
 def log10x10(x) -> np.ndarray:
     x = np.ascontiguousarray(x, dtype=np.float64)
     out = np.zeros_like(x)
-    _check(lib.visqol_b200_log10(_ptr(x), x.size, _ptr(out)))
+    _check(lib.visqol_b200_log10(_dptr(x), x.size, _dptr(out)))
     return out
 
 
@@ -513,8 +595,8 @@ def nsim_table(ref_spec, deg_spec, patch: int, ref_idx, lo, hi) -> np.ndarray:
     lo = np.ascontiguousarray(lo, dtype=np.int64)
     hi = np.ascontiguousarray(hi, dtype=np.int64)
     out = np.zeros(max(1, ri.size * nfd))
-    _check(lib.visqol_b200_nsim_table(_ptr(rs), nfr, _ptr(ds), nfd, nb, patch, ri.size, _i64(ri), _i64(lo),
-                                      _i64(hi), _ptr(out)))
+    _check(lib.visqol_b200_nsim_table(_dptr(rs), nfr, _dptr(ds), nfd, nb, patch, ri.size, _i64(ri), _i64(lo),
+                                      _i64(hi), _dptr(out)))
     return out[: ri.size * nfd].reshape(ri.size, nfd)
 
 
@@ -530,7 +612,7 @@ def dp(sims, lo, hi, static_scratch=False):
     valid = np.zeros(np_, np.uint8)
     reached = c_size_t()
     fn = lib.visqol_b200_dp_static if static_scratch else lib.visqol_b200_dp
-    _check(fn(_ptr(s), np_, nfd, _i64(lo), _i64(hi), _i64(off), valid.ctypes.data_as(POINTER(c_uint8)),
+    _check(fn(_dptr(s), np_, nfd, _i64(lo), _i64(hi), _i64(off), valid.ctypes.data_as(POINTER(c_uint8)),
               ctypes.byref(reached)))
     return off, valid, reached.value
 
@@ -540,12 +622,19 @@ def patch_similarity(ref, deg):
     d = np.ascontiguousarray(deg, dtype=np.float64)
     nr, nc = r.shape
     means, sd, en, mean = np.zeros(nr), np.zeros(nr), np.zeros(nr), c_double()
-    _check(lib.visqol_b200_patch_similarity(_ptr(r), _ptr(d), nr, nc, _ptr(means), _ptr(sd), _ptr(en),
+    _check(lib.visqol_b200_patch_similarity(_dptr(r), _dptr(d), nr, nc, _dptr(means), _dptr(sd), _dptr(en),
                                             ctypes.byref(mean)))
     return mean.value, means, sd, en
 
 
 PENDING = 1
+
+
+def pair_footprint(ref_len: int, deg_len: int, sample_rate: int, mode: int = MODE_AUDIO) -> int:
+    """Upper bound of the device memory one pair takes in a batch (bytes)."""
+    b = c_uint64()
+    _check(lib.visqol_b200_pair_footprint(ref_len, deg_len, sample_rate, mode, ctypes.byref(b)))
+    return b.value
 
 
 class Server:
@@ -646,7 +735,7 @@ def lattice_predict(fvnsim, fvnsim10, fstdnsim, fvdegenergy, model_path: str | N
     arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fvnsim, fvnsim10, fstdnsim, fvdegenergy)]
     mos = c_double()
     _check(lib.visqol_b200_lattice_predict(os.fsencode(model_path) if model_path else None, arrs[0].size,
-                                           *[_ptr(a) for a in arrs], ctypes.byref(mos)))
+                                           *[_dptr(a) for a in arrs], ctypes.byref(mos)))
     return mos.value
 
 

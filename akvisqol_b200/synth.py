@@ -120,8 +120,13 @@ def speech_pair(seed: int, seconds: float = 8.0, sample_rate: int = 16000,
 
 def audio_batch(count: int, seed0: int = SEED_BASE, min_s: float = 3.0, max_s: float = 30.0):
     """Uneven audio pairs: log-uniform lengths, cutoff U(4, 16) kHz, SNR U(10, 40) dB, delay U(0, 200) ms."""
+    return audio_batch_items(range(count), seed0, min_s, max_s)
+
+
+def audio_batch_items(indices, seed0: int = SEED_BASE, min_s: float = 3.0, max_s: float = 30.0):
+    """Items `indices` of audio_batch(count, seed0, min_s, max_s), for any count above them."""
     pairs = []
-    for i in range(count):
+    for i in indices:
         r = _rng(seed0 + 0x10000 + i)
         secs = float(np.exp(r.uniform(np.log(min_s), np.log(max_s))))
         pairs.append(audio_pair(seed0 + i, seconds=secs, cutoff_hz=r.uniform(4000, 16000),

@@ -44,14 +44,31 @@ METRICS = {
     "balanced": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), FP64 FMA form, 1 B200",
     "exact": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), exact FP64 form, 1 B200",
 }
-DTYPES = {"fast": "f32 (gammatone stages 3-4; stages 1-2, lags, NSIM, DP in f64)", "balanced": "f64 (FMA)",
-          "exact": "f64"}
+DTYPES = {"fast": "f32 (gammatone stages 3-4 above the lowest band group, lag-search transform; rescoring, "
+                  "NSIM, DP, MOS in f64)", "balanced": "f64 (FMA)", "exact": "f64"}
 # gammatone: pipe-peak kind of visqol_b200_peak and the algorithm's flops per
 # sample, the same for every form: 4 biquads of 7 flops, the window multiply
 # and the square-accumulate (reference src/gammatone.zig:268-306)
 ROOF = {"exact": (0, 31.0, "fp64-pipe (mul/add)"), "balanced": (1, 31.0, "fp64-pipe (fma)"),
         "fast": (2, 31.0, "fp32-pipe (fma), stages 1-2 on the fp64 pipe")}
 WORKLOAD = "audio-mode pairs, 10 s at 48 kHz (480,000 samples; degraded 481,776), seeded synthetic music-like generator"
+# HBM copy bandwidth of this pool's B200s when the driver's measurement
+# (MEASURED_PEAKS.json) is absent
+HBM_FALLBACK_GBS = 6650.0
+
+
+def hbm_peak() -> tuple[float, str]:
+    """(GB/s, source) of the HBM roofline denominator."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.is_file():
+        try:
+            d = json.loads(f.read_text())
+            for key in ("hbm_gbs", "hbm_GBps", "hbm"):
+                if isinstance(d.get(key), (int, float)) and d[key] > 0:
+                    return float(d[key]), f"of measured (MEASURED_PEAKS.json {key})"
+        except (OSError, ValueError):
+            pass
+    return HBM_FALLBACK_GBS, "of fallback (6.65 TB/s, an earlier copy measurement on this pool)"
 
 
 def parse():
@@ -383,12 +400,21 @@ def isolated_gammatone(native, form: str, ptr_r, ptr_d, len_r, len_d, warmup: in
     launches = sum(t["gammatone_launches"] for t in ts)
     achieved = flops_per_sample * ts[0]["gammatone_window"] * rms / (ms / 1e3) / 1e12 if ms > 0 else None
     peak = native.peak_tflops(kind)
+    lag_ms = sum(t["lag_kernel_ms"] for t in ts)
+    lag_bytes = sum(t["lag_bytes"] for t in ts)
+    hbm, hbm_src = hbm_peak()
+    lag_gbs = lag_bytes / (lag_ms / 1e3) / 1e9 if lag_ms > 0 else None
     del prep, ctx
     return {"achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak if achieved and peak else None,
-            "launches": launches, "rms": rms, "kernel_ms": ms,
-            "how": "one lane, prepared references: the degraded-signal and realignment launches with no other "
-                   "kernel of the step beside them"}
+            "launches": launches, "rms": rms, "kernel_ms": ms, "batches": len(ts),
+            "lag_search": {"bound": "hbm", "achieved": lag_gbs, "peak": hbm, "unit": "GB/s",
+                           "frac": lag_gbs / hbm if lag_gbs else None, "peak_source": hbm_src,
+                           "bytes_per_batch": lag_bytes / len(ts), "kernel_ms_per_batch": lag_ms / len(ts),
+                           "bytes": "signals read (twice in the f32 search: transform and rescoring) + four "
+                                    "passes over the transform buffer (16 B a point in f64, 8 B in f32)"},
+            "how": "one lane, prepared references: the degraded-signal and realignment launches, and the global lag "
+                   "search, with no other kernel of the step beside them; CUDA events around each launch group"}
 
 
 def run_ours(args, rank, world, local):
@@ -508,16 +534,24 @@ def run_ours(args, rank, world, local):
     direct_value = world * B * args.steps / all_max(float(np.sum(direct_times)), world)
     signal_bytes = sum(r.nbytes + d.nbytes for r, d in pairs)
 
-    roof = dict(head["roofline"])
-    roof["measured"] = ("in the timed steps: every lane's launches share the GPU with the other lanes' "
-                        "kernels, so each launch's event-timed span (and this fraction) includes that sharing")
-    roof["isolated"] = isolated_gammatone(native, args.precision, ptr_r, ptr_d, len_r, len_d, args.warmup)
-    roof["traffic"] = None
+    # The dominant kernel (gammatone) on its own: one lane, nothing of the
+    # step beside it, so achieved = algorithmic flops / its own event-timed
+    # duration. The in-step figure (launch spans that include other lanes'
+    # kernels sharing the GPU) is kept under in_step.
+    iso = isolated_gammatone(native, args.precision, ptr_r, ptr_d, len_r, len_d, args.warmup)
+    in_step = dict(head["roofline"])
+    in_step["how"] = ("in the timed steps: every lane's launches share the GPU with the other lanes' kernels, so "
+                      "each launch's event-timed span (and this fraction) includes that sharing")
+    roof = {"bound": in_step["bound"], "kernel": "gammatone", "achieved": iso["achieved"], "peak": iso["peak"],
+            "unit": "TFLOP/s", "frac": iso["frac"], "flops_per_rms": in_step["flops_per_rms"],
+            "peak_source": in_step["peak_source"], "traffic": None,
+            "kernel_ms_per_batch": iso["kernel_ms"] / iso["batches"], "rms_per_batch": iso["rms"] / iso["batches"],
+            "how": iso["how"], "lag_search": iso["lag_search"], "in_step": in_step}
     prof = ROOT / "profiles" / "gammatone_traffic.json"
     if prof.is_file():
         per_rms = json.loads(prof.read_text()).get("dram_bytes_per_rms_audio48k")
         if per_rms:
-            roof["traffic"] = per_rms * head["gt_rms"] / max(1, head["gt_launches"])
+            roof["traffic"] = per_rms * iso["rms"] / max(1, iso["launches"])
     timings = head["timings"]
     stage = {k: float(np.mean([t[k] for t in timings])) for k in
              ("lag_ms", "spectrogram_ms", "prep_ms", "nsim_ms", "realign_ms", "gammatone_kernel_ms", "total_ms")}
@@ -571,6 +605,13 @@ def run_ours(args, rank, world, local):
         cb = cpu_baseline(pairs, args.seconds)
         res = cb.pop("results")
         line["cpu_baseline"] = cb
+        # parity on every pair of the timed batch: the rest of it through the
+        # CPU model too (untimed)
+        if len(res) < len(pairs):
+            import oracle
+            rest = pairs[len(res):]
+            res = res + oracle.measure_batch([p[0] for p in rest], [p[1] for p in rest], 48000,
+                                             threads=os.cpu_count() or 1)
         for f, r in runs.items():
             dmos = [abs(o["moslqo"] - g[1]) for (c, o), g in zip(res, r["results"]) if c == 0 and g[0] == 0]
             line["forms"][f]["max_abs_dmos_vs_oracle"] = max(dmos) if dmos else None

@@ -61,6 +61,9 @@ typedef struct {
     uint64_t kernel_launches;      /* all kernels of the batch */
     uint64_t h2d_bytes, d2h_bytes;
     uint64_t host_syncs;
+    double lag_kernel_ms;          /* the global lag search's kernels, first to last */
+    uint64_t lag_bytes;            /* their algorithmic DRAM bytes (signals, transform passes) */
+    uint64_t lag_reruns;           /* FP32 form: lag searches the f32 pass left undecided */
 } visqol_b200_timing;
 
 /* Score n pairs as visqol_measure_batch does; with traces non-NULL,
@@ -152,6 +155,11 @@ int visqol_b200_server_submit(visqol_b200_server *s, uint32_t mode, const double
 #define VISQOL_B200_PENDING 1
 int visqol_b200_server_next(visqol_b200_server *s, int32_t timeout_ms, uint64_t *ticket, int32_t *status,
                             visqol_result **out);
+/* Device memory one pair of these lengths may take in a batch (an upper
+ * bound of its arena use): the unit of the server's HBM admission. */
+int visqol_b200_pair_footprint(size_t ref_len, size_t deg_len, uint32_t sample_rate, uint32_t mode,
+                               uint64_t *bytes);
+
 /* Counters and latency percentiles; reset != 0 clears the latency samples
  * and the batch counters after reading. The server keeps two doubles per
  * completed request (latency, queueing) until a reset, so a long-running
@@ -205,6 +213,34 @@ int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t
 /* Raw-signal FFT cross-correlation lag (reference src/xcorr.zig:197-251). */
 int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb,
                          int64_t *lag);
+
+/* The lag search of one pair in an arithmetic form: form 0 the exact f64
+ * search (as visqol_b200_envelope_lag / visqol_b200_best_lag), form 1 the
+ * FP32 form's: the correlation in f32, every lag within twice its error
+ * bound of the maximum rescored by f64 dot products, first maximum in
+ * ascending lag (reference refineLag / rescore, src/xcorr.zig:270-340, and
+ * the GPU flow src/gpu/engine.zig:445-540). raw: 1 for the signals
+ * themselves, 0 for their upper envelopes. *undecided (optional) is 1 when
+ * the f32 pass found more than 64 candidates and the exact search decided.
+ * corr (optional, form 1): receives the f32 correlation's real part
+ * (n x the circular cross-correlation, n = fftSizeFor(max(la, lb)) =
+ * corr_len values). */
+int visqol_b200_lag_search(const double *a, size_t la, const double *b, size_t lb, int raw, int form,
+                           int64_t *lag, int32_t *undecided, float *corr, size_t corr_len);
+
+/* refineLag (reference src/xcorr.zig:278-300) on the device: approx[i]
+ * (n values) approximates scale * sum_t s1[t + i] s2[t] (circular index i)
+ * within tol * (|s1|^2 + |s2|^2) * scale; the lags within twice that of
+ * the largest |approx| are rescored by f64 dot products. *decided is 0
+ * (and *lag untouched) when more than 64 qualify, the reference's null. */
+int visqol_b200_refine_lag(const double *s1, size_t l1, const double *s2, size_t l2, const float *approx,
+                           size_t n, double scale, double tol, int64_t *lag, int32_t *decided);
+
+/* out[i] = num[i] / den[i] by the FP32 and FP64-FMA forms' NSIM quotient: a
+ * reciprocal estimate refined by Markstein's Newton-Raphson steps, then one
+ * correction of the quotient. For den[i] > 0 in [2^-1000, 2^1000] the
+ * result is within one ulp of the IEEE quotient. */
+int visqol_b200_nsim_quotient(const double *num, const double *den, size_t n, double *out);
 
 /* Unscaled radix-2 DIF forward (natural in, bit-reversed out) and DIT
  * inverse, in place on n interleaved complex values (reference

@@ -4,11 +4,13 @@
   statistics. It reorders rounding only, so MOS stays within 1e-10 and
   every discrete decision (lags, patch indices, DP offsets, realignment)
   matches.
-* fast: gammatone stages 3-4 in f32. MOS within 1e-6 on the 10 s 48 kHz
-  audio workload; on low-SNR pairs whose upper bands hold flat white noise
-  NSIM's structure term amplifies f32 rounding, and the stated bound there is
-  1e-5. Lags, patch indices (VAD in speech mode) and matched offsets must
-  still be identical.
+* fast: gammatone stages 3-4 in f32 (all four in f64 in the lowest band
+  group, whose poles sit nearest the unit circle). MOS within 1e-6 on every
+  workload: the 10 s 48 kHz audio pairs, the uneven 3-30 s audio batch with
+  its low-SNR pairs (whose widest, noise-only upper bands make NSIM's
+  structure term most sensitive), speech, and other sample rates. Lags,
+  patch indices (VAD in speech mode) and matched offsets must still be
+  identical.
 """
 
 import numpy as np
@@ -54,10 +56,17 @@ def test_audio_10s_48k(native, oracle, contexts, form, tol):
     check(run(contexts[(form, native.MODE_AUDIO)], pairs, 48000), pairs, 48000, oracle, oracle.options(), tol)
 
 
-@pytest.mark.parametrize("form,tol", [("balanced", 1e-10), ("fast", 1e-5)])
+# Items of the 256-pair uneven audio batch (3-30 s, cutoff 4-16 kHz, SNR
+# 10-40 dB): the five whose FP32-form MOS moved most with f32 state in the
+# lowest band group (21: 4.2e-6, 213: 2.3e-6, 7: 2.1e-6, 59: 1.1e-6, 208:
+# 9.8e-7), and three drawn at random.
+UNEVEN_ITEMS = (7, 21, 59, 208, 213, 102, 166, 240)
+
+
+@pytest.mark.parametrize("form,tol", [("balanced", 1e-10), ("fast", 1e-6)])
 def test_uneven_audio(native, oracle, contexts, form, tol):
     from akvisqol_b200 import synth
-    pairs = synth.audio_batch(8, min_s=3.0, max_s=8.0)
+    pairs = synth.audio_batch_items(UNEVEN_ITEMS, min_s=3.0, max_s=30.0)
     check(run(contexts[(form, native.MODE_AUDIO)], pairs, 48000), pairs, 48000, oracle, oracle.options(), tol)
 
 
@@ -82,16 +91,16 @@ def test_batch_equals_single(native, contexts, form):
         assert np.array_equal(res["fvnsim"], res1["fvnsim"])
 
 
-@pytest.mark.parametrize("shape", ["2", "3", "4", "103", "104"])
+@pytest.mark.parametrize("shape", ["2", "102"])
 def test_fast_gammatone_shapes_agree(native, monkeypatch, shape):
-    """Every launch shape of the FP32-form gammatone kernel (register budget of
-    2, 3 or 4 CTAs per SM; one CTA per tile, or a persistent grid taking tiles
-    from a device-side work queue) gives the same bits."""
+    """Both launch shapes of the FP32-form gammatone kernel (one CTA per tile,
+    or a persistent grid taking tiles from a device-side work queue) give the
+    same bits."""
     from akvisqol_b200 import synth
     pairs = synth.audio_batch(5, seed0=synth.SEED_BASE + 700, min_s=2.0, max_s=6.0)
     refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
     ctx = native.Context(mode=native.MODE_AUDIO, precision="fast")
-    monkeypatch.setenv("VISQOL_TUNE_3", "3")
+    monkeypatch.setenv("VISQOL_TUNE_3", "2")
     base = ctx.measure_batch_traced(refs, degs, 48000)
     monkeypatch.setenv("VISQOL_TUNE_3", shape)
     got = ctx.measure_batch_traced(refs, degs, 48000)
@@ -156,7 +165,7 @@ def _rate_case(oracle, sr):
 
 
 @pytest.mark.parametrize("sr", [44100, 22050])
-@pytest.mark.parametrize("form,tol", [("exact", 1e-12), ("balanced", 1e-10), ("fast", 1e-5)])
+@pytest.mark.parametrize("form,tol", [("exact", 1e-12), ("balanced", 1e-10), ("fast", 1e-6)])
 def test_other_sample_rates(native, oracle, sr, form, tol):
     """Audio mode at 44.1 and 22.05 kHz: windows of 3528 and 1764 samples,
     not multiples of the staged gammatone kernels' 64-sample tiles, so each

@@ -106,7 +106,7 @@ def test_batch_equals_single(native, audio_ctx):
     pairs = [synth.audio_pair(synth.SEED_BASE + i, seconds=3.0) for i in range(3)]
     batch = run(audio_ctx, pairs, 48000)
     for (ref, deg), (code, res, tr) in zip(pairs, batch):
-        single = native.result_dict(audio_ctx.measure(native.as_signal(ref, "r"), native.as_signal(deg, "d"), 48000).contents)
+        single = native.result_dict(audio_ctx.measure(native.mono(ref, "r"), native.mono(deg, "d"), 48000).contents)
         assert res["moslqo"] == single["moslqo"]
         assert np.array_equal(res["fvnsim"], single["fvnsim"])
 
@@ -218,7 +218,7 @@ def test_autotune_choices_are_candidates(native, audio_ctx):
             assert r["choice"] in (0, 1)  # shared-memory tiles, registers
         elif r["kernel"] == "gammatone_fast_shape":
             # FP32-form kernel: CTAs per SM, + 100 for the persistent work-queue form
-            assert r["choice"] in (2, 3, 4, 103, 104)
+            assert r["choice"] in (2, 102)
         elif r["kernel"] == "gammatone_f64_staged":
             assert r["choice"] in (0, 1)  # FP64-FMA kernel, or the same form on staged tiles
         else:

@@ -100,3 +100,31 @@ def test_pending_when_idle(native):
     server = native.Server(precision="exact", lanes=1)
     assert server.next(timeout_ms=10) is None
     server.close()
+
+
+def test_pooled_budget_admits_pair_larger_than_a_lane_share(native):
+    """HBM is one pool: with four lanes and a budget of 1.5 footprints, a pair
+    of one footprint (more than a quarter of the budget) is admitted, each in
+    turn, and scores as it does alone; a pair larger than the whole budget is
+    refused."""
+    from akvisqol_b200 import synth
+    pairs = [synth.audio_pair(synth.SEED_BASE + 60 + i, seconds=6.0) for i in range(3)]
+    foot = max(native.pair_footprint(r.size, d.size, 48000) for r, d in pairs)
+    server = native.Server(precision="exact", lanes=4, max_batch=8, hbm_budget_bytes=foot * 3 // 2)
+    tickets = {server.submit(0, r, d, 48000): k for k, (r, d) in enumerate(pairs)}
+    got = {}
+    for _ in pairs:
+        t, status, res = server.next(timeout_ms=120000)
+        assert status == 0
+        got[tickets[t]] = res
+    st = server.stats()
+    assert st["completed"] == 3 and st["failed"] == 0 and st["mean_batch"] == 1.0
+    big = synth.audio_pair(synth.SEED_BASE + 70, seconds=12.0)
+    assert native.pair_footprint(big[0].size, big[1].size, 48000) > foot * 3 // 2
+    with pytest.raises(native.NativeError) as e:
+        server.submit(0, big[0], big[1], 48000)
+    assert e.value.code == native.E_OUT_OF_MEMORY
+    server.close()
+    for k, (r, d) in enumerate(pairs):
+        want = _alone(native, "exact", 0, (r, d), 48000)
+        assert got[k]["moslqo"] == want["moslqo"]
