@@ -71,14 +71,32 @@ class _T:
         return None if v is None else self.buf[v[0]:v[0] + v[1]].decode()
 
 
+def _fma32(p: float, q: float, c: float) -> np.float32:
+    """fmaf(p, q, c) exactly, for f32 values given as floats: p*q is exact in
+    f64; the f64 sum s = p*q + c and its error e (TwoSum, exact) give the
+    exact result s + e. Rounding s to f32 equals rounding s + e unless s sits
+    exactly on a midpoint between two f32 values and e != 0; then the
+    neighbour on e's side is the correctly rounded result."""
+    prod = p * q
+    s = prod + c
+    bb = s - prod
+    e = (prod - (s - bb)) + (c - bb)
+    r = np.float32(s)
+    fr = float(r)
+    if e != 0.0 and fr != s:
+        other = np.nextafter(r, np.float32(np.inf) if s > fr else np.float32(-np.inf))
+        if float(other) - s == s - fr:  # s is the midpoint of r and other
+            up = e > 0.0
+            r = max(r, other) if up else min(r, other)
+    return np.float32(r)
+
+
 def _fma_dot(x: np.ndarray, w: np.ndarray) -> np.float32:
-    """Sequential f32 FMA from zero: each step rounds (p*q + acc) once to
-    f32 (p*q of two f32 values is exact in f64; the f64 sum is rounded once
-    more, which can differ from a true FMA in rare double-rounding cases)."""
-    acc = np.float32(0.0)
-    for p, q in zip(x.astype(np.float64), w.astype(np.float64)):
-        acc = np.float32(p * q + np.float64(acc))
-    return acc
+    """Sequential f32 FMA from zero, each step rounded once to f32."""
+    acc = 0.0
+    for p, q in zip(x.astype(np.float64).tolist(), w.astype(np.float64).tolist()):
+        acc = float(_fma32(p, q, acc))
+    return np.float32(acc)
 
 
 class Lattice:

@@ -165,5 +165,8 @@ def main(ref_root: Path, out: Path) -> None:
 
 
 if __name__ == "__main__":
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-    main(root, Path(__file__).with_name("reference_kats.json"))
+    import os
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VISQOL_REFERENCE_ROOT")
+    if not where:
+        sys.exit("usage: make_reference_kats.py <reference checkout> (or set VISQOL_REFERENCE_ROOT)")
+    main(Path(where), Path(__file__).with_name("reference_kats.json"))

@@ -90,10 +90,12 @@ def test_speech_lattice_is_reported(native):
     assert e.value.code in (native.E_MODEL, native.E_BACKEND)
 
 
-REFERENCE_PY = Path("/root/reference/src/python")
+# The reference's src/python directory, when a checkout is at hand.
+REFERENCE_PY = Path(os.environ.get("VISQOL_REFERENCE_PYTHON", "/nonexistent"))
 
 
-@pytest.mark.skipif(not REFERENCE_PY.is_dir(), reason="reference Python package not present")
+@pytest.mark.skipif(not (REFERENCE_PY / "visqol" / "_native.py").is_file(),
+                    reason="VISQOL_REFERENCE_PYTHON does not name the reference's src/python")
 def test_reference_python_package_loads_this_library(native):
     """The reference's own binding (src/python/visqol/_native.py) loads
     libvisqol.so through VISQOL_LIBRARY unchanged."""
