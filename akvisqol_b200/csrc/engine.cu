@@ -348,7 +348,20 @@ int32_t *Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw, bool exact
                     j.rescore = rescore + (size_t)kLagCandCap * nchunks * k;
                     chunk[k] = j;
                 }
-                launch_lag32(upload(chunk), (int)cnt, n, raw, tw.cols32, tw.block32, tw.stages32, nchunks, stream_);
+                LagJob *d_chunk = upload(chunk);
+                auto launch32 = [&](int columns) {
+                    launch_lag32(d_chunk, (int)cnt, n, raw, tw.cols32, tw.block32, tw.stages32, nchunks, columns,
+                                 stream_);
+                };
+                // forward samples staged in shared memory, or loaded into
+                // registers: measured per transform size
+                const char *env = std::getenv("VISQOL_LAG_COLUMNS");
+                const int columns = !fused_lag_register_columns(n) ? 0
+                                    : env && (env[0] == '0' || env[0] == '1' || env[0] == '2')
+                                        ? env[0] - '0'
+                                        : tuned(kTuneLagColumns, (int)std::log2((double)n), raw ? 3 : 2, {2, 1},
+                                                launch32, stream_);
+                launch32(columns);
                 continue;
             }
             // (above 2^24 points the exact search decides in every form; status stays 0)
@@ -366,15 +379,16 @@ int32_t *Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw, bool exact
                 auto launch = [&](int columns) {
                     launch_fused_lag(d_jobs, (int)cnt, n, raw, tw.cols, tw.block, tw.stages, pv, pk, columns, stream_);
                 };
-                // column passes: shared-memory tiles or registers, measured per
-                // transform size (VISQOL_LAG_COLUMNS=0/1 fixes the choice)
+                // column passes: shared-memory tiles, registers, or registers
+                // with the forward samples staged, measured per transform size
+                // (VISQOL_LAG_COLUMNS=0/1/2 fixes the choice)
                 int columns = 0;
                 if (fused_lag_register_columns(n)) {
                     const char *env = std::getenv("VISQOL_LAG_COLUMNS");
-                    columns = env && (env[0] == '0' || env[0] == '1')
+                    columns = env && (env[0] == '0' || env[0] == '1' || env[0] == '2')
                                   ? env[0] - '0'
-                                  : tuned(kTuneLagColumns, (int)std::log2((double)n), raw ? 1 : 0, {1, 0}, launch,
-                                          stream_);
+                                  : tuned(kTuneLagColumns, (int)std::log2((double)n), raw ? 1 : 0, {1, 2, 0},
+                                          launch, stream_);
                 }
                 launch(columns);
                 continue;

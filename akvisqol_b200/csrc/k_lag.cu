@@ -118,12 +118,12 @@ __device__ inline EnvParams env_params(const VSig &s, const double *stats) {
 }
 
 // upperEnvelope (reference src/envelope.zig:45-52) at sample i.
-__device__ inline double env_at(const VSig &s, const EnvParams &p, int64_t i) {
-    const double x = vsig_at(s, i);
+__device__ inline double env_of(double x, const EnvParams &p, int64_t i) {
     const double pc = x - p.mean;
     const double nt = (i & 1) ? -p.q : p.q;
     return fabs(2.0 * (pc - nt) - 0.000001) + p.mean;
 }
+__device__ inline double env_at(const VSig &s, const EnvParams &p, int64_t i) { return env_of(vsig_at(s, i), p, i); }
 
 template <bool RAW>
 __device__ inline double2 packed(const LagJob &job, const EnvParams &pa, const EnvParams &pb, int64_t i) {
@@ -135,6 +135,17 @@ __device__ inline double2 packed(const LagJob &job, const EnvParams &pa, const E
 
 // Point i of z in the search's type; the f32 search also sums the squares
 // of the f64 envelope values (its nomination slack scales with them).
+template <class C>
+__device__ inline C as_point(double2 v, double &ea, double &eb) {
+    if constexpr (std::is_same<C, float2>::value) {
+        ea += v.x * v.x;
+        eb += v.y * v.y;
+        return make_float2((float)v.x, (float)v.y);
+    } else {
+        return v;
+    }
+}
+
 template <class C, bool RAW>
 __device__ inline C pack_point(const LagJob &job, const EnvParams &pa, const EnvParams &pb, int64_t i, double &ea,
                                double &eb) {
@@ -759,6 +770,88 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_columns_reg(const LagJob *__r
     store_energy<C>(job, ea, eb);
 }
 
+// 8-byte asynchronous copy to shared memory; `in` false writes zeros (no
+// bytes are read; src must still be a global address).
+__device__ inline void cp_async8z(double *dst, const double *src, bool in) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(in ? 8 : 0) : "memory");
+}
+
+// Pass 1 as fwd_columns_reg, with the CTA's 4096 (a, b) samples first staged
+// in shared memory by asynchronous copies (16 a thread, consecutive threads
+// on consecutive columns of a row, zero outside the stored samples): every
+// load is in flight at once and none holds a register, where the register
+// form's loads queue behind its 128-register budget. The values, and so the
+// results, are the register form's. The stage is then the exchange buffer.
+template <class C, int G, bool RAW>
+__global__ void __launch_bounds__(kThreads, 2) fwd_columns_staged(const LagJob *__restrict__ jobs,
+                                                               const C *__restrict__ tcol) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *sm = reinterpret_cast<C *>(smem_raw);
+    double2 *stage = reinterpret_cast<double2 *>(smem_raw);  // [row][col] of the tile
+    constexpr int R = 1 << G, cols = kB >> G;
+    const LagJob job = jobs[blockIdx.y];
+    const int c = threadIdx.x % cols, q = threadIdx.x / cols;
+    const int64_t c0 = (int64_t)blockIdx.x * cols, col = c0 + c;
+    C *z = zbuf<C>(job);
+    const double *guard = reinterpret_cast<const double *>(z);
+#pragma unroll
+    for (int k = 0; k < kB / kThreads; ++k) {
+        const int e = threadIdx.x + k * kThreads;
+        const int t = e / cols, cc = e - t * cols;
+        const int64_t i = (int64_t)t * kB + c0 + cc;
+        const int64_t ja = i - job.a.head, jb = i - job.b.head;
+        const bool ina = i < job.a.len && (uint64_t)ja < (uint64_t)job.a.avail;
+        const bool inb = i < job.b.len && (uint64_t)jb < (uint64_t)job.b.avail;
+        cp_async8z(&stage[e].x, ina ? job.a.base + ja : guard, ina);
+        cp_async8z(&stage[e].y, inb ? job.b.base + jb : guard, inb);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    EnvParams pa{}, pb{};
+    if (!RAW) {
+        pa = env_params(job.a, job.stats_a);
+        pb = env_params(job.b, job.stats_b);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    C x[16];
+    double ea = 0.0, eb = 0.0;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int64_t i = (int64_t)row_a<G>(q, m) * kB + col;
+        const double2 v = stage[row_a<G>(q, m) * cols + c];
+        double re = 0.0, im = 0.0;
+        if (i < job.a.len) re = RAW ? v.x : env_of(v.x, pa, i);
+        if (i < job.b.len) im = RAW ? v.y : env_of(v.y, pb, i);
+        x[m] = as_point<C>(make_double2(re, im), ea, eb);
+    }
+    __syncthreads();  // the stage becomes the exchange buffer
+    column_group4<C, G, false>(x, 0, R / 16, q, tcol, col);
+    if (G > 4) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) sm[row_a<G>(q, m) * cols + c] = x[m];
+        __syncthreads();
+        if (G > 8) {
+            constexpr int s = R / 256 > 0 ? R / 256 : 1;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) x[m] = sm[row_b<G>(q, m) * cols + c];
+            column_group4<C, G, false>(x, 4, s, q % s, tcol, col);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) sm[row_b<G>(q, m) * cols + c] = x[m];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = sm[row_t(q, m) * cols + c];
+        column_tail<C, G, false>(x, G > 8 ? 8 : 4, tcol, col);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) z[(int64_t)row_t(q, m) * kB + col] = x[m];
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) z[(int64_t)row_a<G>(q, m) * kB + col] = x[m];
+    }
+    store_energy<C>(job, ea, eb);
+}
+
 template <int G>
 __global__ void __launch_bounds__(kThreads, 2) inv_columns_reg(const LagJob *__restrict__ jobs,
                                                             const double2 *__restrict__ tcol, double *pv,
@@ -1180,7 +1273,12 @@ void lag_init_attributes() {
 #define VQB_COLS_ATTR(GG)                                                                                 \
     cudaFuncSetAttribute(fwd_columns_reg<double2, GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);  \
     cudaFuncSetAttribute(fwd_columns_reg<double2, GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+    cudaFuncSetAttribute(fwd_columns_staged<double2, GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+    cudaFuncSetAttribute(fwd_columns_staged<double2, GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+    cudaFuncSetAttribute(fwd_columns_staged<float2, GG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
+    cudaFuncSetAttribute(fwd_columns_staged<float2, GG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, one); \
     cudaFuncSetAttribute(inv_columns_reg<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+    VQB_COLS_ATTR(4)
     VQB_COLS_ATTR(5)
     VQB_COLS_ATTR(6)
     VQB_COLS_ATTR(7)
@@ -1249,11 +1347,18 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
     const int64_t nblk = n / kB;
     const dim3 grid((unsigned)parts, (unsigned)njobs);
     const size_t reg_smem = G > 4 ? one : 0;
-    const int Gr = columns == 1 ? G : 0;  // 0: no register pass, the shared-memory one
+    // 0: the shared-memory column passes; 1: register passes; 2: register
+    // passes with the forward samples staged in shared memory
+    const int Gr = columns == 1 || columns == 2 ? G : 0;
+    const bool staged = columns == 2;
     switch (Gr) {
 #define VQB_COLS(GG)                                                                                       \
     case GG:                                                                                               \
-        if (raw)                                                                                           \
+        if (staged && raw)                                                                                 \
+            fwd_columns_staged<double2, GG, true><<<grid, kThreads, one, s>>>(d_jobs, tcol);               \
+        else if (staged)                                                                                   \
+            fwd_columns_staged<double2, GG, false><<<grid, kThreads, one, s>>>(d_jobs, tcol);              \
+        else if (raw)                                                                                      \
             fwd_columns_reg<double2, GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);             \
         else                                                                                               \
             fwd_columns_reg<double2, GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);            \
@@ -1323,7 +1428,7 @@ int lag32_rescore_chunks(int64_t max_b_len) {
 }
 
 void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const float2 *tcol, const float2 *tw_block,
-                  const float2 *tst, int nchunks, cudaStream_t s) {
+                  const float2 *tst, int nchunks, int columns, cudaStream_t s) {
     if (njobs <= 0) return;
     const int parts = (int)lag32_parts(n);
     if (n <= kB) {
@@ -1340,11 +1445,18 @@ void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const fl
         const dim3 grid((unsigned)parts, (unsigned)njobs);
         const size_t one = (size_t)kB * sizeof(float2);
         const size_t reg_smem = G > 4 ? one : 0;
-        const int Gr = fused_lag_register_columns(n) ? G : 0;
+        const size_t stage_smem = (size_t)kB * sizeof(double2);
+        // as launch_fused_lag: 1 register passes, 2 with staged forward samples
+        const int Gr = fused_lag_register_columns(n) && columns != 0 ? G : 0;
+        const bool staged = columns == 2;
         switch (Gr) {
 #define VQB_COLS32(GG)                                                                                     \
     case GG:                                                                                               \
-        if (raw)                                                                                           \
+        if (staged && raw)                                                                                 \
+            fwd_columns_staged<float2, GG, true><<<grid, kThreads, stage_smem, s>>>(d_jobs, tcol);         \
+        else if (staged)                                                                                   \
+            fwd_columns_staged<float2, GG, false><<<grid, kThreads, stage_smem, s>>>(d_jobs, tcol);        \
+        else if (raw)                                                                                      \
             fwd_columns_reg<float2, GG, true><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);              \
         else                                                                                               \
             fwd_columns_reg<float2, GG, false><<<grid, kThreads, reg_smem, s>>>(d_jobs, tcol);             \

@@ -121,7 +121,9 @@ void fill_column_twiddles(const double2 *top, int64_t n, double2 *out);
 size_t block_stage_twiddle_count();
 void fill_block_stage_twiddles(const double2 *block, double2 *out);
 // columns: 0 = the shared-memory column passes (any n), 1 = the register
-// ones (only where fused_lag_register_columns(n); else as 0). Same results.
+// ones, 2 = the register ones with the forward pass's samples staged in
+// shared memory (1 and 2 only where fused_lag_register_columns(n); else as
+// 0). Same results.
 bool fused_lag_register_columns(int64_t n);
 void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const double2 *tcol,
                       const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
@@ -138,7 +140,7 @@ void lag32_init_attributes();
 size_t lag32_parts(int64_t n);
 int lag32_rescore_chunks(int64_t max_b_len);
 void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const float2 *tcol, const float2 *tw_block,
-                  const float2 *tst, int nchunks, cudaStream_t s);
+                  const float2 *tst, int nchunks, int columns, cudaStream_t s);  // columns as launch_fused_lag's
 // The nomination, pick and rescoring kernels on one job's caller-supplied
 // approximate correlation (corr_out, n values) with slack_fixed as the slack,
 // raw signals; the job's cands array holds ceil(n / 4096) records.

@@ -63,12 +63,13 @@ def test_lags_random(native, oracle):
         assert native.envelope_lag(a, b) == oracle.envelope_lag(a, b)
 
 
-@pytest.mark.parametrize("columns", ["0", "1"])
+@pytest.mark.parametrize("columns", ["0", "1", "2"])
 @pytest.mark.parametrize("rows_log2", [3, 4, 5, 6, 7, 8, 9, 10, 11])
 def test_lags_column_pass_sizes(native, oracle, rows_log2, columns, monkeypatch):
     """Signal lengths whose transforms have 2^rows_log2 rows of 4096 points,
     with each column-pass implementation: shared-memory tiles (0) and, for
-    4..11 rows_log2, registers (1)."""
+    4..11 rows_log2, registers (1) and registers with the forward pass's
+    samples staged in shared memory (2)."""
     monkeypatch.setenv("VISQOL_LAG_COLUMNS", columns)
     n = 4096 << rows_log2
     rng = np.random.default_rng(100 + rows_log2)

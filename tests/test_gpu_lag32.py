@@ -130,3 +130,21 @@ def test_fast_lag_undecided_falls_back(native, oracle, kind):
         assert lag == want, (kind, raw, lag, want)
         if kind != "periodic":
             assert undecided == 1
+
+
+@pytest.mark.parametrize("columns", ["0", "1", "2"])
+@pytest.mark.parametrize("rows_log2", [1, 3, 4, 6, 8, 9, 11])
+def test_fast_lags_column_pass_shapes(native, oracle, rows_log2, columns, monkeypatch):
+    """The f32 search with each column-pass shape (shared-memory tiles;
+    registers; registers with the forward samples staged) at transforms of
+    2^rows_log2 rows of 4096 points: the exact search's lag."""
+    monkeypatch.setenv("VISQOL_LAG_COLUMNS", columns)
+    n = 4096 << rows_log2
+    rng = np.random.default_rng(300 + rows_log2)
+    la = int(0.4 * n)
+    a = rng.uniform(-1, 1, la)
+    shift = int(rng.integers(1, 400))
+    b = np.concatenate([np.zeros(shift), a])[:la + 57] + 0.05 * rng.standard_normal(la + 57)
+    for raw in (True, False):
+        want = oracle.best_lag(a, b) if raw else oracle.envelope_lag(a, b)
+        assert native.lag_search(a, b, raw=raw, form="fast")[0] == want
