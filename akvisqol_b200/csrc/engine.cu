@@ -723,7 +723,7 @@ void Engine::lags(size_t njobs, const VSig *a, const VSig *b, bool raw, int64_t 
 }
 
 bool Engine::refine_approx(const VSig &a, const VSig &b, const float *d_approx, int64_t n, double slack,
-                           int64_t *lag) {
+                           double energy, int64_t *lag) {
     arena_.reset();
     pinned_.reset();
     LagJob j{};
@@ -736,6 +736,9 @@ bool Engine::refine_approx(const VSig &a, const VSig &b, const float *d_approx, 
     j.corr_out = const_cast<float *>(d_approx);
     j.slack_fixed = slack;
     j.cands = arena_.alloc_n<LagCands>(parts);
+    std::vector<double2> e(parts, make_double2(0.0, 0.0));
+    e[0].x = energy;  // the rescoring's tie margin scales with it
+    j.energy = upload(e);
     j.status = arena_.alloc_n<int32_t>(1);
     j.ncand = arena_.alloc_n<int32_t>(1);
     j.cand_key = arena_.alloc_n<int32_t>(kLagCandCap);

@@ -172,8 +172,10 @@ public:
               float *d_corr = nullptr);
     // The f32 search's nomination and f64 rescoring on a caller-supplied
     // approximate correlation of raw signals a and b (n values, device),
-    // with the given slack. Returns false when it leaves the lag undecided.
-    bool refine_approx(const VSig &a, const VSig &b, const float *d_approx, int64_t n, double slack, int64_t *lag);
+    // with the given slack; energy = |a|^2 + |b|^2. Returns false when it
+    // leaves the lag undecided.
+    bool refine_approx(const VSig &a, const VSig &b, const float *d_approx, int64_t n, double slack, double energy,
+                       int64_t *lag);
     // FFT twiddles of size n on the device: the full table and the block
     // passes' compact one (cached per size).
     struct Twiddles {

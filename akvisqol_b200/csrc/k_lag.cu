@@ -1242,25 +1242,54 @@ __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__r
     }
 }
 
+// Rescored candidates closer than this fraction of |a|^2 + |b|^2 are a tie
+// as far as the two searches can tell: each search's rounding error is
+// below 1e-13 of it, real lags' differences are far above.
+constexpr double kTieMargin = 1e-10;
+
+// The best |dot| so far (value, lag key) and the second best value.
+struct Top2 {
+    Best first;
+    double second;
+};
+__device__ inline bool prefers(Best x, Best y) { return x.v > y.v || (x.v == y.v && x.key < y.key); }
+__device__ inline Top2 merge(Top2 a, Top2 b) {
+    if (prefers(b.first, a.first)) return Top2{b.first, fmax(b.second, a.first.v)};
+    return Top2{a.first, fmax(a.second, b.first.v)};
+}
+
 // The first maximum of |dot| in ascending lag (reference rescore
-// src/xcorr.zig:311-325). One warp per job.
-__global__ void pick_rescored(const LagJob *__restrict__ jobs, int njobs, int nchunks) {
+// src/xcorr.zig:311-325). Where the two best are within kTieMargin (a
+// periodic signal's equal peaks), which of them the exact search picks is
+// decided by its own rounding, so the job is left to it (status 1). One
+// warp per job; parts: the job's energy records.
+__global__ void pick_rescored(const LagJob *__restrict__ jobs, int njobs, int nchunks, int parts) {
     const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (j >= njobs) return;
     const LagJob job = jobs[j];
     if (*job.status != 0) return;
     const int count = *job.ncand;
-    Best best{-INFINITY, INT64_MAX};
+    double e = 0.0;
+    for (int p = lane; p < parts; p += 32) e += job.energy[p].x + job.energy[p].y;
+    for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+    e = __shfl_sync(0xffffffffu, e, 0);
+    Top2 top{Best{-INFINITY, INT64_MAX}, -INFINITY};
     for (int c = lane; c < count; c += 32) {
         double d = 0.0;
         for (int k = 0; k < nchunks; ++k) d += job.rescore[(int64_t)c * nchunks + k];
-        best = better(best, Best{fabs(d), (int64_t)job.cand_key[c]});
+        top = merge(top, Top2{Best{fabs(d), (int64_t)job.cand_key[c]}, -INFINITY});
     }
     for (int off = 16; off > 0; off >>= 1) {
-        Best o{__shfl_down_sync(0xffffffffu, best.v, off), __shfl_down_sync(0xffffffffu, best.key, off)};
-        best = better(best, o);
+        Top2 o{Best{__shfl_down_sync(0xffffffffu, top.first.v, off), __shfl_down_sync(0xffffffffu, top.first.key, off)},
+               __shfl_down_sync(0xffffffffu, top.second, off)};
+        top = merge(top, o);
     }
-    if (lane == 0) *job.lag_out = best.key - (job.biggest - 1);
+    if (lane == 0) {
+        if (top.first.v - top.second <= kTieMargin * e)
+            *job.status = 1;
+        else
+            *job.lag_out = top.first.key - (job.biggest - 1);
+    }
 }
 
 }  // namespace
@@ -1406,7 +1435,7 @@ void launch_refine_approx(const LagJob *d_job, int64_t n, int nchunks, cudaStrea
     nominate_approx<<<parts, kThreads, 0, s>>>(d_job);
     pick_candidates<<<1, kThreads, 0, s>>>(d_job, parts);
     rescore_candidates<true><<<dim3((unsigned)nchunks, 1), kThreads, 0, s>>>(d_job, nchunks);
-    pick_rescored<<<1, 32, 0, s>>>(d_job, 1, nchunks);
+    pick_rescored<<<1, 32, 0, s>>>(d_job, 1, nchunks, parts);
     launch_counter() += 4;
 }
 
@@ -1502,7 +1531,7 @@ void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const fl
         rescore_candidates<true><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
     else
         rescore_candidates<false><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
-    pick_rescored<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, nchunks);
+    pick_rescored<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, nchunks, parts);
     launch_counter() += 3;
 }
 

@@ -145,7 +145,7 @@ int visqol_b200_refine_lag(const double *s1, size_t l1, const double *s2, size_t
         DBuf<double> da(s1, l1), db(s2, l2);
         DBuf<float> dx(approx, n);
         const vqb::VSig va{da.p, 0, (int64_t)l1, (int64_t)l1}, vb{db.p, 0, (int64_t)l2, (int64_t)l2};
-        *decided = stage_engine(vqb::kFormF32).refine_approx(va, vb, dx.p, (int64_t)n, slack, lag) ? 1 : 0;
+        *decided = stage_engine(vqb::kFormF32).refine_approx(va, vb, dx.p, (int64_t)n, slack, e1 + e2, lag) ? 1 : 0;
     });
 }
 
