@@ -375,19 +375,20 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
 // least-loaded lane, lanes run concurrently, outcomes gathered back in order.
 void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, std::vector<vqb::PairOutcome> &res,
-               const vqb::PreparedRef *const *prepared = nullptr) {
+               const vqb::PreparedRef *const *prepared = nullptr, bool grads = false) {
     const size_t L = std::min(c->lanes.size(), std::max<size_t>(1, n));
     res.assign(n, vqb::PairOutcome{});
     // Host inputs: uploads overlap scoring, through the shared chunk queue
-    // when the batch splits, else lane by lane.
-    const bool streamed = !device_inputs && vqb::env_streamed_uploads();
+    // when the batch splits, else lane by lane (gradients: signals uploaded
+    // whole, the gradient pass reads them after scoring).
+    const bool streamed = !device_inputs && !grads && vqb::env_streamed_uploads();
     if (streamed && run_lanes_queued(c, n, refs, ref_lens, degs, deg_lens, sample_rate, res, prepared)) return;
     auto measure = [&](vqb::Engine &e, size_t m, const double *const *r, const size_t *rl, const double *const *d,
                        const size_t *dl, std::vector<vqb::PairOutcome> &o, const vqb::PreparedRef *const *pr) {
         if (streamed)
             e.measure_batch_streamed(m, r, rl, d, dl, sample_rate, o, pr);
         else
-            e.measure_batch(m, r, rl, d, dl, sample_rate, device_inputs, o, pr);
+            e.measure_batch(m, r, rl, d, dl, sample_rate, device_inputs, o, pr, nullptr, grads);
     };
     if (L <= 1) {
         measure(*c->lanes[0], n, refs, ref_lens, degs, deg_lens, res, prepared);
@@ -453,6 +454,9 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
         t.h2d_bytes += x.h2d_bytes;
         t.d2h_bytes += x.d2h_bytes;
         t.host_syncs += x.host_syncs;
+        t.lag_kernel_ms = std::max(t.lag_kernel_ms, x.lag_kernel_ms);
+        t.lag_bytes += x.lag_bytes;
+        t.lag_reruns += x.lag_reruns;
     }
     c->timing = t;
 }
@@ -460,10 +464,11 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
 // One batch through the engine with per-pair results and status.
 int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
               const size_t *deg_lens, uint32_t sample_rate, bool device_inputs, visqol_result **out, int32_t *status,
-              visqol_b200_trace **traces, const vqb::PreparedRef *const *prepared = nullptr) {
+              visqol_b200_trace **traces, const vqb::PreparedRef *const *prepared = nullptr,
+              double *const *grads = nullptr) {
     std::vector<vqb::PairOutcome> res;
     try {
-        run_lanes(c, n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res, prepared);
+        run_lanes(c, n, refs, ref_lens, degs, deg_lens, sample_rate, device_inputs, res, prepared, grads != nullptr);
     } catch (const Error &e) {
         for (size_t i = 0; i < n; ++i) {
             out[i] = nullptr;
@@ -482,6 +487,8 @@ int run_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *
         if (traces) traces[i] = nullptr;
         int rc = res[i].code;
         if (rc == VISQOL_OK) {
+            if (grads && grads[i] && res[i].grad.size() == deg_lens[i])
+                std::copy(res[i].grad.begin(), res[i].grad.end(), grads[i]);
             out[i] = vqb::box_result(std::move(res[i].scores));
             if (traces) traces[i] = box_trace(std::move(res[i].trace));
         } else {
@@ -731,6 +738,17 @@ int visqol_measure_files_batch(visqol_ctx *c, size_t n, const char *const *ref_p
 void visqol_result_free(visqol_result *r) {
     if (!r) return;
     delete reinterpret_cast<Box *>(r);
+}
+
+int visqol_b200_measure_batch_grad(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,
+                                   const double *const *degs, const size_t *deg_lens, uint32_t sample_rate,
+                                   uint32_t flags, visqol_result **out, int32_t *status, double *const *grads) {
+    if (!c) return fail(VISQOL_E_INVALID_ARGUMENT, "ctx is NULL");
+    if (n == 0) return VISQOL_OK;
+    if (!out || !grads) return fail(VISQOL_E_INVALID_ARGUMENT, "out or grads is NULL");
+    if (!refs || !degs || !ref_lens || !deg_lens) return fail(VISQOL_E_INVALID_ARGUMENT, "NULL signal table");
+    return run_batch(c, n, refs, ref_lens, degs, deg_lens, sample_rate, (flags & VISQOL_B200_DEVICE_INPUTS) != 0, out,
+                     status, nullptr, nullptr, grads);
 }
 
 int visqol_b200_measure_batch(visqol_ctx *c, size_t n, const double *const *refs, const size_t *ref_lens,

@@ -77,6 +77,16 @@ struct LagJob {
     double slack_fixed;  // test only (else 0): the nomination slack, instead of the f32 error bound
 };
 
+// One spectrogram's reverse (k_grad.cu): d loss / d RMS cells g_rms[b * nf +
+// f] of the frames of `sig` to d loss / d samples, added to grad[k - head]
+// for the stored samples (grad indexed as sig.base).
+struct GradSpecJob {
+    VSig sig;
+    int64_t nf;
+    const double *g_rms;
+    double *grad;
+};
+
 // Serial reductions over a signal, in the CPU's order, into
 // out[0] = sum x, out[1] = sum (-1)^k (x - mean), out[2] = sum x*x.
 struct SumJob {

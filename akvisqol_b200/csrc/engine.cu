@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "grad_host.h"
 #include "kernels.h"
 
 namespace vqb {
@@ -777,7 +778,7 @@ void Engine::spectrogram(const host::Filterbank &fb, const double *d_hann, size_
     sync();
 }
 
-namespace {
+namespace detail {
 
 struct RealignPatch {
     size_t mi;
@@ -803,6 +804,8 @@ struct PairState {
     double *stats = nullptr;  // device: ref[4], deg[4], aligned energy, aligned length
     host::Aligned al{};
     double factor = 1.0;
+    double al_energy = 0.0;  // energy of the aligned degraded signal (its SPL)
+    double ref_energy = 0.0;
     size_t nf_ref = 0, nf_deg = 0;
     std::vector<int64_t> idx;
     host::Search search;
@@ -814,6 +817,7 @@ struct PairState {
     uint8_t *valid = nullptr;
     double *mstats = nullptr;
     std::vector<host::Match> matches;
+    bool grad_ok = false;  // scored, and its gradient requested
     std::vector<RealignPatch> rps;
     PairTrace trace;
     void fail(int c, const std::string &m) {
@@ -823,12 +827,15 @@ struct PairState {
     }
 };
 
-}  // namespace
+}  // namespace detail
+
+using detail::PairState;
+using detail::RealignPatch;
 
 void Engine::measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                            const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
                            std::vector<PairOutcome> &out, const PreparedRef *const *prepared,
-                           const double *const *host_refs) {
+                           const double *const *host_refs, bool grads) {
     out.assign(n, PairOutcome{});
     timing_ = Timing{};
     if (n == 0) return;
@@ -1027,6 +1034,8 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                                                  : host::apply_lag_geometry(s.rl, s.dl, lag, sample_rate);
             const double *st = h_stats + 10 * i;
             s.factor = host::spl_factor(st[2], s.rl, st[8], (size_t)s.al.len);
+            s.al_energy = st[8];
+            s.ref_energy = st[2];
             s.trace.spl_factor = s.factor;
             s.trace.deg_len = (uint64_t)s.al.len;
             if (s.rl <= W || (size_t)s.al.len <= W) throw Error(kSignal, "SpectrogramTooShort");
@@ -1378,6 +1387,11 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
     } else {
         for (size_t i = 0; i < n; ++i) finish(i);
     }
+    if (grads) {
+        for (size_t i = 0; i < n; ++i)
+            if (ps[i].live && out[i].code == 0) ps[i].grad_ok = true;
+        gradients(ps.data(), n, deg_lens, rc, out);
+    }
     timing_.total_ms = elapsed(events_[0], events_[7]);
     timing_.lag_ms = elapsed(events_[0], events_[1]);
     timing_.spectrogram_ms = elapsed(events_[2], events_[3]);
@@ -1519,6 +1533,172 @@ void Engine::measure_batch_streamed(size_t n, const double *const *refs, const s
     }
     sum.h2d_bytes += h2d;
     timing_ = sum;
+}
+
+}  // namespace vqb
+
+namespace vqb {
+
+void Engine::gradients(detail::PairState *ps, size_t n, const size_t *deg_lens, const RateCache &rc,
+                       std::vector<PairOutcome> &out) {
+    const size_t NB = nb_, P = patch_, W = rc.geo.window, H = rc.geo.hop;
+    const double fd = rc.geo.frame_duration;
+    // 1. the raw spectrograms the statistics came from, and the degraded samples
+    struct HostCopy {
+        std::vector<double> ref, deg, sig;
+        std::vector<std::vector<double>> rs, ds;  // per realignment patch
+    };
+    std::vector<HostCopy> hc(n);
+    auto fetch = [&](std::vector<double> &dst, const double *src, size_t count) {
+        dst.resize(count);
+        if (count) VQB_CUDA(cudaMemcpyAsync(dst.data(), src, count * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        timing_.d2h_bytes += count * sizeof(double);
+    };
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.grad_ok) continue;
+        HostCopy &h = hc[i];
+        fetch(h.ref, s.ref_raw, NB * s.nf_ref);
+        fetch(h.deg, s.deg_raw, NB * s.nf_deg);
+        fetch(h.sig, s.deg, s.dl);
+        h.rs.resize(s.rps.size());
+        h.ds.resize(s.rps.size());
+        for (size_t k = 0; k < s.rps.size(); ++k)
+            if (s.rps[k].nf) {
+                fetch(h.rs[k], s.rps[k].rs_raw, NB * s.rps[k].nf);
+                fetch(h.ds[k], s.rps[k].ds_raw, NB * s.rps[k].nf);
+            }
+    }
+    sync();
+
+    // 2. host reverses: MOS -> match statistics -> prepared cells -> raw
+    // degraded cells, for the global spectrograms and each accepted
+    // realignment slice
+    std::vector<std::vector<double>> g_glob(n);
+    struct SliceGrad {
+        size_t pair, rp;
+        std::vector<double> g;
+    };
+    std::vector<SliceGrad> slice_grads;
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.grad_ok) continue;
+        const HostCopy &h = hc[i];
+        const std::vector<host::Match> &matches = out[i].scores.patches;
+        const PairTrace &tr = out[i].trace;
+        const size_t nfr = s.nf_ref, nfd = s.nf_deg;
+        std::vector<host::MatchGrad> mg;
+        host::scores_grad(matches, NB, fd, svr_.get(), opt_.speech, opt_.unscaled_speech, lattice_.get(), mg);
+        std::vector<double> rprep, dprep;
+        host::prepare_forward(h.ref.data(), h.deg.data(), NB, nfr, nfd, rprep, dprep);
+        std::vector<double> g_ref(NB * nfr, 0.0), g_deg(NB * nfd, 0.0);
+        g_glob[i].assign(NB * nfd, 0.0);
+        std::vector<double> pr(NB * P), pd(NB * P), dr(NB * P), dd(NB * P);
+        for (size_t p = 0; p < matches.size(); ++p) {
+            if (!tr.valid[p] || tr.deg_offset[p] < 0) continue;  // statistics are constants
+            const host::MatchGrad &g = mg[p];
+            if (tr.realign_accepted[p]) {
+                size_t k = 0;
+                while (k < s.rps.size() && !(s.rps[k].mi == p && s.rps[k].nf)) ++k;
+                if (k == s.rps.size()) continue;
+                const RealignPatch &rp = s.rps[k];
+                const size_t nf = rp.nf;
+                std::vector<double> a, b, da(NB * nf, 0.0), db(NB * nf, 0.0), gds(NB * nf, 0.0);
+                host::prepare_forward(h.rs[k].data(), h.ds[k].data(), NB, nf, nf, a, b);
+                host::patch_similarity_grad(a.data(), b.data(), NB, nf, g.dmeans.data(), g.dstddevs.data(),
+                                            g.denergy.data(), da.data(), db.data());
+                host::prepare_grad(h.rs[k].data(), h.ds[k].data(), NB, nf, nf, da.data(), db.data(), gds.data());
+                if (rp.reused & 2) {
+                    // the slice's degraded frames were the global spectrogram's
+                    const int64_t g0 = host::reuse_frame(rp.dl, rp.trim.deg_off, H, nf, nfd);
+                    for (size_t bb = 0; bb < NB; ++bb)
+                        for (size_t f = 0; f < nf; ++f) g_glob[i][bb * nfd + g0 + f] += gds[bb * nf + f];
+                } else {
+                    slice_grads.push_back(SliceGrad{i, k, std::move(gds)});
+                }
+                continue;
+            }
+            const size_t idx = (size_t)tr.ref_index[p], off = (size_t)tr.deg_offset[p];
+            for (size_t bb = 0; bb < NB; ++bb)
+                for (size_t c = 0; c < P; ++c) {
+                    pr[bb * P + c] = rprep[bb * nfr + idx + c];
+                    pd[bb * P + c] = off + c < nfd ? dprep[bb * nfd + off + c] : 0.0;
+                }
+            std::fill(dr.begin(), dr.end(), 0.0);
+            std::fill(dd.begin(), dd.end(), 0.0);
+            host::patch_similarity_grad(pr.data(), pd.data(), NB, P, g.dmeans.data(), g.dstddevs.data(),
+                                        g.denergy.data(), dr.data(), dd.data());
+            for (size_t bb = 0; bb < NB; ++bb)
+                for (size_t c = 0; c < P; ++c) {
+                    g_ref[bb * nfr + idx + c] += dr[bb * P + c];
+                    if (off + c < nfd) g_deg[bb * nfd + off + c] += dd[bb * P + c];
+                }
+        }
+        host::prepare_grad(h.ref.data(), h.deg.data(), NB, nfr, nfd, g_ref.data(), g_deg.data(), g_glob[i].data());
+    }
+
+    // 3. the gammatone reverse on the device, into each pair's gradient with
+    // respect to its scaled, aligned degraded signal
+    std::vector<GradSpecJob> jobs;
+    std::vector<double *> d_g(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.grad_ok) continue;
+        d_g[i] = arena_.alloc_n<double>((size_t)s.al.len);
+        launch_zero(d_g[i], (size_t)s.al.len * sizeof(double), stream_);
+        jobs.push_back(GradSpecJob{VSig{s.deg_al, 0, s.al.len, s.al.len}, (int64_t)s.nf_deg, upload(g_glob[i]), d_g[i]});
+    }
+    for (const SliceGrad &sg : slice_grads) {
+        PairState &s = ps[sg.pair];
+        const RealignPatch &rp = s.rps[sg.rp];
+        jobs.push_back(GradSpecJob{VSig{s.deg_al + rp.dl.base, rp.dl.pad - rp.trim.deg_off, rp.dl.len, rp.trim.len},
+                                   (int64_t)rp.nf, upload(sg.g), d_g[sg.pair] + rp.dl.base});
+    }
+    if (!jobs.empty()) {
+        const int F = gammatone_bwd_frames_per_cta();
+        const size_t tsz = gammatone_tile_size();
+        std::vector<char> tiles;
+        int ntiles = 0;
+        for (size_t j = 0; j < jobs.size(); ++j)
+            for (int64_t f = 0; f < jobs[j].nf; f += F, ++ntiles) {
+                tiles.resize(tiles.size() + tsz);
+                fill_gammatone_tile(tiles.data() + tiles.size() - tsz, (int)j, (int)f);
+            }
+        const GradSpecJob *d_jobs = upload(jobs);
+        const void *d_tiles = upload_bytes(tiles.data(), tiles.size());
+        double *scratch = arena_.alloc_n<double>(gammatone_bwd_scratch_count(ntiles, (int)W));
+        launch_gammatone_bwd(d_jobs, d_tiles, ntiles, rc.d_fast_coeffs, (int)NB, rc.d_hann, (int)W, (int)H, scratch,
+                             stream_);
+    }
+    std::vector<std::vector<double>> g_al(n);
+    for (size_t i = 0; i < n; ++i)
+        if (ps[i].grad_ok) fetch(g_al[i], d_g[i], (size_t)ps[i].al.len);
+    sync();
+
+    // 4. the SPL scaling (scaled = factor x aligned, factor ~ |aligned|^-1)
+    // and the lag (aligned[i] = deg[i - lead + skip]) reversed
+    for (size_t i = 0; i < n; ++i) {
+        PairState &s = ps[i];
+        if (!s.grad_ok) continue;
+        const std::vector<double> &x = hc[i].sig, &g = g_al[i];
+        const int64_t lead = s.al.lead, skip = s.al.skip, L = s.al.len;
+        auto aligned = [&](int64_t k) {
+            const int64_t d = k - lead + skip;
+            return k >= lead && d >= 0 && d < (int64_t)s.dl ? x[(size_t)d] : 0.0;
+        };
+        const double f = s.factor, E = s.al_energy;
+        const bool depends = s.ref_energy > 0.0 && E > 0.0 && s.rl > 0 && L > 0;
+        double dldf = 0.0;
+        if (depends)
+            for (int64_t k = 0; k < L; ++k) dldf += g[(size_t)k] * aligned(k);
+        std::vector<double> &gd = out[i].grad;
+        gd.assign(deg_lens[i], 0.0);
+        for (int64_t k = lead; k < L; ++k) {
+            const int64_t d = k - lead + skip;
+            if (d < 0 || d >= (int64_t)s.dl) continue;
+            gd[(size_t)d] = f * g[(size_t)k] - (depends ? dldf * f * aligned(k) / E : 0.0);
+        }
+    }
 }
 
 }  // namespace vqb

@@ -18,6 +18,10 @@
 
 namespace vqb {
 
+namespace detail {
+struct PairState;  // one pair's state through measure_batch (engine.cu)
+}
+
 struct Options {
     bool speech = false;
     int32_t radius = 60;
@@ -43,6 +47,7 @@ struct PairOutcome {
     std::string message;
     host::Scores scores;
     PairTrace trace;
+    std::vector<double> grad;  // d moslqo / d degraded sample (deg_len), when requested
 };
 
 // Algorithmic DRAM bytes of one lag search (f32: the FP32 form's search).
@@ -132,10 +137,12 @@ public:
     // reference from there (refs[i] and ref_lens[i] are ignored).
     // host_refs (device inputs only, may be NULL): host copies of the
     // references, read by the speech-mode VAD instead of a read-back.
+    // grads: also d moslqo / d degraded signal of each pair scored
+    // (PairOutcome::grad), the forward's discrete decisions fixed.
     void measure_batch(size_t n, const double *const *refs, const size_t *ref_lens, const double *const *degs,
                        const size_t *deg_lens, uint32_t sample_rate, bool device_inputs,
                        std::vector<PairOutcome> &out, const PreparedRef *const *prepared = nullptr,
-                       const double *const *host_refs = nullptr);
+                       const double *const *host_refs = nullptr, bool grads = false);
     // Host inputs scored in consecutive chunks of growing size: chunk k+1's
     // signals are copied to the device on a copy stream (from a helper
     // thread, so pageable sources do not block scoring) while chunk k is
@@ -213,6 +220,12 @@ private:
     uint64_t launch_spectrograms(const std::vector<SpecJob> &jobs, const RateCache &rc, cudaStream_t st,
                                  cudaEvent_t begin = nullptr, cudaEvent_t end = nullptr);
     const RateCache &rate_cache(uint32_t sample_rate);
+    // d moslqo / d degraded signal of the pairs measure_batch just scored
+    // (grad_ok), into out[i].grad: the host reverses of the MOS mapping,
+    // NSIM statistics and spectrogram preparation, the gammatone reverse on
+    // the device, then the SPL scaling's and the lag's reverses on the host.
+    void gradients(detail::PairState *ps, size_t n, const size_t *deg_lens, const RateCache &rc,
+                   std::vector<PairOutcome> &out);
 
     // Envelope (or raw) lag search for jobs whose a/b/stat pointers are set;
     // lags land in the jobs' lag_out (device). Launches only. The FP32 form

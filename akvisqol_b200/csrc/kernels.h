@@ -182,6 +182,14 @@ void launch_gammatone_f64_staged(const SpecJob *d_jobs, const void *d_tiles, int
                                  const FastBandCoeffs *d_coeffs, int nb, const double *d_hann, int window, int hop,
                                  cudaStream_t s);
 
+// k_grad.cu: the gammatone spectrogram's reverse (FP64-FMA arithmetic).
+// Tiles as fill_gammatone_tile writes them, of gammatone_bwd_frames_per_cta()
+// frames; d_scratch holds gammatone_bwd_scratch_count(ntiles, window) doubles.
+int gammatone_bwd_frames_per_cta();
+size_t gammatone_bwd_scratch_count(int ntiles, int window);
+void launch_gammatone_bwd(const GradSpecJob *d_jobs, const void *d_tiles, int ntiles, const FastBandCoeffs *d_coeffs,
+                          int nb, const double *d_hann, int window, int hop, double *d_scratch, cudaStream_t s);
+
 // k_spec.cu
 // Spectrogram preparation of njobs pairs (max_frames = the largest nfr or
 // nfd); d_scratch holds prep_scratch_count(njobs, max_frames) doubles.

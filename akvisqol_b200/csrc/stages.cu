@@ -11,6 +11,7 @@
 
 #include "../../include/visqol_b200.h"
 #include "engine.h"
+#include "grad_host.h"
 #include "host_model.h"
 #include "kernels.h"
 
@@ -158,6 +159,31 @@ int visqol_b200_nsim_quotient(const double *num, const double *den, size_t n, do
         VQB_CUDA(cudaStreamSynchronize(e.stream()));
         dq.get(out, n);
     });
+}
+
+int visqol_b200_patch_similarity_grad(const double *ref, const double *deg, size_t nrows, size_t ncols,
+                                      const double *dmeans, const double *dstddevs, const double *denergy,
+                                      double *dref, double *ddeg) {
+    if (!ref || !deg || !dref || !ddeg || nrows == 0 || ncols == 0)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    try {
+        vqb::host::patch_similarity_grad(ref, deg, nrows, ncols, dmeans, dstddevs, denergy, dref, ddeg);
+    } catch (const std::exception &e) {
+        return stage_fail(VISQOL_E_INTERNAL, e.what());
+    }
+    return VISQOL_OK;
+}
+
+int visqol_b200_prepare_grad(const double *ref_raw, const double *deg_raw, size_t nb, size_t nfr, size_t nfd,
+                             const double *g_ref, const double *g_deg, double *g_deg_raw) {
+    if (!ref_raw || !deg_raw || !g_ref || !g_deg || !g_deg_raw || nb == 0)
+        return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    try {
+        vqb::host::prepare_grad(ref_raw, deg_raw, nb, nfr, nfd, g_ref, g_deg, g_deg_raw);
+    } catch (const std::exception &e) {
+        return stage_fail(VISQOL_E_INTERNAL, e.what());
+    }
+    return VISQOL_OK;
 }
 
 int visqol_b200_fft(double *buf, size_t n, int inverse) {

@@ -137,6 +137,9 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_measure_batch": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, POINTER(c_void_p), SZ,
                                               c_uint32, c_uint32, POINTER(POINTER(Result)), POINTER(c_int32),
                                               POINTER(POINTER(Trace))]),
+        "visqol_b200_measure_batch_grad": (c_int, [c_void_p, c_size_t, POINTER(c_void_p), SZ, POINTER(c_void_p), SZ,
+                                                   c_uint32, c_uint32, POINTER(POINTER(Result)), POINTER(c_int32),
+                                                   POINTER(c_void_p)]),
         "visqol_b200_trace_free": (None, [POINTER(Trace)]),
         "visqol_b200_last_timing": (c_int, [c_void_p, POINTER(Timing)]),
         "visqol_b200_device_info": (c_int, [c_int, c_char_p, c_size_t, POINTER(c_int), POINTER(c_int),
@@ -150,6 +153,8 @@ def _load() -> ctypes.CDLL:
                                            I64, POINTER(c_int32)]),
         "visqol_b200_fft": (c_int, [D, c_size_t, c_int]),
         "visqol_b200_nsim_quotient": (c_int, [D, D, c_size_t, D]),
+        "visqol_b200_patch_similarity_grad": (c_int, [D, D, c_size_t, c_size_t, D, D, D, D, D]),
+        "visqol_b200_prepare_grad": (c_int, [D, D, c_size_t, c_size_t, c_size_t, D, D, D]),
         "visqol_b200_prepare_for_comparison": (c_int, [D, D, c_size_t, c_size_t, c_size_t]),
         "visqol_b200_log10": (c_int, [D, c_size_t, D]),
         "visqol_b200_nsim_table": (c_int, [D, c_size_t, D, c_size_t, c_size_t, c_size_t, c_size_t, I64, I64, I64, D]),
@@ -193,9 +198,10 @@ EXPORTS = [
     "visqol_abi_version", "visqol_version", "visqol_last_error", "visqol_available_backends",
     "visqol_options_default", "visqol_create", "visqol_destroy", "visqol_measure", "visqol_measure_files",
     "visqol_measure_batch", "visqol_measure_files_batch", "visqol_result_free",
-    "visqol_b200_measure_batch", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
+    "visqol_b200_measure_batch", "visqol_b200_measure_batch_grad", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
     "visqol_b200_spectrogram", "visqol_b200_envelope_lag", "visqol_b200_best_lag", "visqol_b200_fft",
     "visqol_b200_lag_search", "visqol_b200_refine_lag", "visqol_b200_nsim_quotient",
+    "visqol_b200_patch_similarity_grad", "visqol_b200_prepare_grad",
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
     "visqol_b200_dp_static",
     "visqol_b200_patch_similarity", "visqol_b200_peak",
@@ -431,6 +437,27 @@ class Context:
                 got.append((int(status[i]), None, None))
         return got
 
+    def measure_batch_grad(self, refs, degs, sample_rate: int):
+        """Scores with d moslqo / d degraded signal: per pair ``(code,
+        result dict or None, gradient array or None)``."""
+        n = len(refs)
+        r, d = _Signals(refs), _Signals(degs)
+        grads = [np.zeros(a.size) for a in d.hold]
+        gp = (c_void_p * n)(*[g.ctypes.data for g in grads])
+        outs, status = (POINTER(Result) * n)(), (c_int32 * n)()
+        rc = lib.visqol_b200_measure_batch_grad(self._handle, n, r.ptrs, r.lens, d.ptrs, d.lens, sample_rate, 0, outs,
+                                                status, gp)
+        if rc and all(int(status[i]) == OK for i in range(n)):
+            raise error_for(rc)
+        got = []
+        for i in range(n):
+            if int(status[i]) == OK:
+                got.append((OK, result_dict(outs[i].contents), grads[i]))
+                free(outs[i])
+            else:
+                got.append((int(status[i]), None, None))
+        return got
+
     def last_timing(self) -> dict:
         t = Timing()
         _check(lib.visqol_b200_last_timing(self._handle, ctypes.byref(t)))
@@ -563,6 +590,32 @@ def nsim_quotient(num, den) -> np.ndarray:
         raise ValueError("num and den differ in length")
     out = np.empty(num.size)
     _check(lib.visqol_b200_nsim_quotient(_dptr(num), _dptr(den), num.size, _dptr(out)))
+    return out
+
+
+def patch_similarity_grad(ref, deg, dmeans=None, dstddevs=None, denergy=None):
+    """Host reverse of the patch statistics: (dref, ddeg), each ref.shape."""
+    ref = np.ascontiguousarray(ref, dtype=np.float64)
+    deg = np.ascontiguousarray(deg, dtype=np.float64)
+    nr, nc = ref.shape
+    dref, ddeg = np.zeros_like(ref), np.zeros_like(deg)
+    opt = [None if v is None else mono(v) for v in (dmeans, dstddevs, denergy)]
+    _check(lib.visqol_b200_patch_similarity_grad(_dptr(ref), _dptr(deg), nr, nc,
+                                                 *[None if v is None else _dptr(v) for v in opt],
+                                                 _dptr(dref), _dptr(ddeg)))
+    return dref, ddeg
+
+
+def prepare_grad(ref_raw, deg_raw, g_ref, g_deg) -> np.ndarray:
+    """Host reverse of prepareForComparison: d loss / d raw degraded cells."""
+    ref_raw = np.ascontiguousarray(ref_raw, dtype=np.float64)
+    deg_raw = np.ascontiguousarray(deg_raw, dtype=np.float64)
+    g_ref = np.ascontiguousarray(g_ref, dtype=np.float64)
+    g_deg = np.ascontiguousarray(g_deg, dtype=np.float64)
+    nb, nfr = ref_raw.shape
+    out = np.zeros_like(deg_raw)
+    _check(lib.visqol_b200_prepare_grad(_dptr(ref_raw), _dptr(deg_raw), nb, nfr, deg_raw.shape[1], _dptr(g_ref),
+                                        _dptr(g_deg), _dptr(out)))
     return out
 
 

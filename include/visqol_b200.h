@@ -76,6 +76,22 @@ int visqol_b200_measure_batch(visqol_ctx *ctx, size_t n,
                               visqol_result **out, int32_t *status,
                               visqol_b200_trace **traces);
 void visqol_b200_trace_free(visqol_b200_trace *trace);
+
+/* Scores n pairs as visqol_b200_measure_batch does and also d moslqo / d
+ * degraded signal of each (reference backend.Engine.measureBatchGrad,
+ * src/backend.zig:101-109): grads[i], a host buffer of deg_lens[i]
+ * doubles (NULL: pair i's gradient is skipped), receives the gradient with
+ * respect to each degraded sample. The forward pass's discrete choices are
+ * held fixed: the global and per-patch lags, the patch matches and the
+ * realignment decisions, and which cells the spectrogram floors and the
+ * joint minimum select. Where the MOS mapping is clamped the gradient is
+ * zero. The speech lattice mapper's own gradient is by central
+ * differences over its features, as the reference's. */
+int visqol_b200_measure_batch_grad(visqol_ctx *ctx, size_t n,
+                                   const double *const *refs, const size_t *ref_lens,
+                                   const double *const *degs, const size_t *deg_lens,
+                                   uint32_t sample_rate, uint32_t flags,
+                                   visqol_result **out, int32_t *status, double *const *grads);
 int visqol_b200_last_timing(visqol_ctx *ctx, visqol_b200_timing *out);
 
 /* ---- prepared references ---------------------------------------------------
@@ -241,6 +257,23 @@ int visqol_b200_refine_lag(const double *s1, size_t l1, const double *s2, size_t
  * correction of the quotient. For den[i] > 0 in [2^-1000, 2^1000] the
  * result is within one ulp of the IEEE quotient. */
 int visqol_b200_nsim_quotient(const double *num, const double *den, size_t n, double *out);
+
+/* Reverse of measurePatchSimilarity (reference src/nsim.zig:427-510), on the
+ * host: for nrows x ncols prepared ref and deg cells and the gradients with
+ * respect to the patch's band means, standard deviations and deg energies
+ * (each nrows values, or NULL for zero), accumulates the gradients with
+ * respect to the cells into dref and ddeg. */
+int visqol_b200_patch_similarity_grad(const double *ref, const double *deg, size_t nrows, size_t ncols,
+                                      const double *dmeans, const double *dstddevs, const double *denergy,
+                                      double *dref, double *ddeg);
+
+/* Reverse of prepareForComparison (reference src/spectrogram.zig:69-80), on
+ * the host: from the raw spectrograms (nb x nfr, nb x nfd) and the
+ * gradients with respect to the prepared cells, accumulates the gradient
+ * with respect to the raw degraded cells into g_deg_raw. The cells the
+ * floors and the joint minimum select are those of the forward pass. */
+int visqol_b200_prepare_grad(const double *ref_raw, const double *deg_raw, size_t nb, size_t nfr, size_t nfd,
+                             const double *g_ref, const double *g_deg, double *g_deg_raw);
 
 /* Unscaled radix-2 DIF forward (natural in, bit-reversed out) and DIT
  * inverse, in place on n interleaved complex values (reference
