@@ -489,7 +489,7 @@ __device__ inline void dit16(C (&x)[16], int j, const C *__restrict__ tst) {
 }
 
 template <class C>
-__global__ void __launch_bounds__(kMidThreads, 1) middle_blocks(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kMidThreads, sizeof(C) == 8 ? 2 : 1) middle_blocks(const LagJob *__restrict__ jobs,
                                                                 const C *__restrict__ tst) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
