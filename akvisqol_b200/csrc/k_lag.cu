@@ -1212,7 +1212,10 @@ constexpr int kRescoreChunk = 4096;  // b samples per rescoring CTA
 // Partial dot products sum_j a[j + lag] b[j] of every candidate lag over
 // this CTA's chunk of b (reference dotAtLag src/xcorr.zig:328-340; the
 // summation order is this kernel's, fixed), of the envelopes (or raw
-// signals), in f64. grid (chunks, jobs).
+// signals), in f64. Up to kRescoreGroup candidates (usually neighbouring
+// lags) share one pass over the chunk: b's value is formed once, a's for
+// each lag hit the same cache lines. grid (chunks, jobs).
+constexpr int kRescoreGroup = 8;
 template <bool RAW>
 __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__restrict__ jobs, int nchunks) {
     const LagJob job = jobs[blockIdx.y];
@@ -1225,20 +1228,33 @@ __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__r
     }
     const int64_t max_lag = job.biggest - 1;
     const int64_t j0 = (int64_t)blockIdx.x * kRescoreChunk;
-    for (int c = 0; c < count; ++c) {
-        const int64_t lag = (int64_t)job.cand_key[c] - max_lag;
-        double acc = 0.0;
-#pragma unroll 4
+    for (int c0 = 0; c0 < count; c0 += kRescoreGroup) {
+        const int cn = count - c0 < kRescoreGroup ? count - c0 : kRescoreGroup;
+        int64_t lag[kRescoreGroup];
+        double acc[kRescoreGroup];
+#pragma unroll
+        for (int g = 0; g < kRescoreGroup; ++g) {
+            lag[g] = g < cn ? (int64_t)job.cand_key[c0 + g] - max_lag : 0;
+            acc[g] = 0.0;
+        }
+#pragma unroll 2
         for (int k = 0; k < kRescoreChunk / kThreads; ++k) {
-            const int64_t j = j0 + threadIdx.x + k * kThreads, ia = j + lag;
-            if (j < job.b.len && ia >= 0 && ia < job.a.len) {
-                const double x = RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia);
-                const double y = RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j);
-                acc += x * y;
+            const int64_t j = j0 + threadIdx.x + k * kThreads;
+            if (j >= job.b.len) continue;
+            const double y = RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j);
+#pragma unroll
+            for (int g = 0; g < kRescoreGroup; ++g) {
+                const int64_t ia = j + lag[g];
+                if (g < cn && ia >= 0 && ia < job.a.len) {
+                    const double x = RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia);
+                    acc[g] += x * y;
+                }
             }
         }
-        acc = block_sum(acc);
-        if (threadIdx.x == 0) job.rescore[(int64_t)c * nchunks + blockIdx.x] = acc;
+        for (int g = 0; g < cn; ++g) {
+            const double t = block_sum(acc[g]);
+            if (threadIdx.x == 0) job.rescore[(int64_t)(c0 + g) * nchunks + blockIdx.x] = t;
+        }
     }
 }
 
