@@ -3,11 +3,13 @@
 //
 // The reference sums signals left to right in f64 (envelope mean and
 // Nyquist term, src/envelope.zig:28-41; SPL energy, src/audio.zig:132-136).
-// A parallel tree would round differently, so each reduction runs as one
-// warp per signal: the warp loads tiles of consecutive samples (coalesced),
-// forms the per-sample terms in parallel into shared memory, and then adds
-// them in index order. The f64 add chain is the only serial part; many
-// signals run side by side.
+// A parallel tree would round differently, so each reduction is one warp per
+// signal that reproduces the serial sum's every rounding: tiles of samples
+// are staged in shared memory, the sums of x and x*x advance a whole tile at
+// a time by an exact integer form of the serial additions (exact_prefix)
+// and fall back to adding term by term where it does not apply; the
+// alternating Nyquist sum is added term by term. Many signals run side by
+// side.
 #include "device.cuh"
 #include "kernels.h"
 
@@ -21,104 +23,204 @@ enum SumKind : int {
     kEnergy = 2,        // out[2] = sum x*x
 };
 
-// Samples per tile: each lane loads 8 (coalesced 256-byte rows), forms the
-// per-sample terms, and writes them to this warp's shared-memory tile;
-// then every lane walks the tile in index order adding broadcast reads, so
-// the only serial dependency left is the f64 add itself. The next tile's
-// global loads are in flight meanwhile (double buffering).
+// Tiles of 256 consecutive samples move into this warp's shared-memory
+// stages by asynchronous copies (each lane 8 samples of coalesced 256-byte
+// rows; zeros outside the stored window), kStages tiles in flight. In a
+// stage, the 8 samples k = 8L .. 8L+7 of the tile sit at L * kPad + (k & 7):
+// lane L reads its own run without bank conflicts, and all lanes read any
+// one sample as a broadcast.
 constexpr int kRows = 8;
 constexpr int kTile = 32 * kRows;
-constexpr int kSerialWarps = 4;
+constexpr int kPad = kRows + 1;
+constexpr int kSlots = 32 * kPad;
+constexpr int kStages = 8;
+constexpr int kSerialWarps = 2;
 
-template <int KIND>
-__device__ inline void tile_terms(double v, int64_t k, double mean, double &t0, double &t1) {
-    if (KIND == kSumAndEnergy) {
-        t0 = v;
-        t1 = v * v;
-    } else if (KIND == kNyquist) {
-        const double d = v - mean;
-        t0 = (k & 1) ? -d : d;
+__device__ inline int slot_of(int i) { return (i >> 3) * kPad + (i & 7); }
+
+__device__ double g_copy_guard;  // source address of the zero-filling copies
+
+// 8-byte asynchronous copy to shared memory; `in` false writes zeros.
+__device__ inline void copy8(double *dst, const double *src, bool in) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(in ? src : &g_copy_guard),
+                 "r"(in ? 8 : 0)
+                 : "memory");
+}
+
+// Exact shortcut for a serial f64 sum (the CPU's `s += t`, left to right).
+// While the running sum stays in one binade [2^e, 2^(e+1)), every value it
+// takes is a multiple of u = 2^(e-52), and s + t rounds to the multiple of u
+// nearest the exact value, s + u * rint(t / u), unless t / u is a
+// half-integer (a tie, which round-half-even settles by the parity of s). A
+// tile of terms is then added as integers: q = rint(t / u) per term, a
+// prefix sum over the warp, and a check that every partial sum M (in units
+// of u) stays a unit inside the binade, 2^52 + 1 <= M <= 2^53 - 2, so that
+// the exact value of each addition, within half a unit of u * M, lies in the
+// binade as well. The first term that breaks a condition ends the shortcut:
+// the sum before it is exact, and the caller adds the rest one at a time.
+// t: this lane's terms (tile index 8 * lane + j); left: the tile's terms.
+// Returns how many leading terms were added into s (the same in all lanes).
+__device__ inline int exact_prefix(double &s, const double (&t)[kRows], int left) {
+    const int lane = threadIdx.x & 31;
+    const long long bits = __double_as_longlong(s);
+    const int e = (int)((bits >> 52) & 0x7ff);
+    // zero, subnormal or below 2^-970 (the unit scales below must be
+    // normal), infinite or NaN: no shortcut
+    if (e < 53 || e == 0x7ff) return 0;
+    const double to_units = __longlong_as_double((long long)(2098 - e) << 52);  // 1 / u
+    const double from_units = __longlong_as_double((long long)(e - 52) << 52);  // u
+    const bool neg = bits < 0;
+    long long run[kRows];
+    long long acc = 0;
+    unsigned ok = 0;
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+        // a power-of-two scale is exact (a result far below 1/2 may round,
+        // but rounds to q = 0 either way)
+        const double tau = neg ? -(t[j] * to_units) : t[j] * to_units;
+        const double q = rint(tau);
+        const bool good = fabs(q) <= 0x1p53 && fabs(tau - q) != 0.5;  // NaN and inf fail the first test
+        acc += good ? (long long)q : 0;
+        run[j] = acc;
+        ok |= (unsigned)good << j;
+    }
+    long long incl = acc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const long long base = ((bits & ((1LL << 52) - 1)) | (1LL << 52)) + (incl - acc);
+    int first = kTile;
+#pragma unroll
+    for (int j = kRows - 1; j >= 0; --j) {
+        const long long m = base + run[j];
+        const bool bad = !((ok >> j) & 1u) || m < (1LL << 52) + 1 || m > (1LL << 53) - 2;
+        if (bad && lane * kRows + j < left) first = lane * kRows + j;
+    }
+    int k = __reduce_min_sync(0xffffffffu, first);
+    k = k < left ? k : left;
+    if (k > 0) {
+        const int last = k - 1, js = last & (kRows - 1);
+        long long mine = 0;
+#pragma unroll
+        for (int j = 0; j < kRows; ++j)
+            if (j == js) mine = base + run[j];
+        const long long m = __shfl_sync(0xffffffffu, mine, last >> 3);
+        const double v = (double)m * from_units;  // m < 2^53: exact
+        s = neg ? -v : v;
+    }
+    return k;
+}
+
+// acc += stage terms from .. to - 1, in index order (every lane the same).
+__device__ inline void serial_add(double &acc, const double *st, int from, int to) {
+    if (from == 0 && to == kTile) {
+#pragma unroll 8
+        for (int g = 0; g < 32; ++g) {
+            const double *p = st + g * kPad;
+            double v[kRows];
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) v[j] = p[j];
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) acc += v[j];
+        }
     } else {
-        t0 = v * v;
+#pragma unroll 8
+        for (int i = from; i < to; ++i) acc += st[slot_of(i)];
     }
 }
 
 // Left-to-right sums, in index order, of KIND's per-sample terms over
 // sample(start + k), k in [0, n): chain 0 (and chain 1 for kSumAndEnergy).
-// tiles: this warp's 2 (buffers) x 2 (chains) x kTile doubles.
+// Sums of x and x*x take the exact integer shortcut tile by tile; the
+// alternating Nyquist sum, whose running value changes binade every few
+// samples, is added one term at a time from the staged terms.
+// stages: this warp's kStages * kSlots doubles. first_nz (kSumAndEnergy):
+// the first k whose x*x is nonzero, n if none.
 template <int KIND>
 __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, double mean, double &acc0,
-                                   double &acc1, double *tiles, int64_t *first_nz = nullptr) {
+                                   double &acc1, double *stages, int64_t *first_nz = nullptr) {
     const int lane = threadIdx.x & 31;
-    double reg[kRows];
-    int64_t nz = n;  // kSumAndEnergy: this lane's first index whose x*x is nonzero
-    auto load = [&](int64_t base) {
+    if (n <= 0) return;
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    auto issue = [&](int64_t t) {
+        if (t < ntiles) {
+            double *st = stages + (int)(t % kStages) * kSlots;
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            const int64_t k = base + r * 32 + lane;
-            reg[r] = k < n ? vsig_at(sig, start + k) : 0.0;
-        }
-    };
-    auto store = [&](int64_t base, int buf) {
-        double *c0 = tiles + buf * 2 * kTile, *c1 = c0 + kTile;
-#pragma unroll
-        for (int r = 0; r < kRows; ++r) {
-            double t0, t1 = 0.0;
-            tile_terms<KIND>(reg[r], base + r * 32 + lane, mean, t0, t1);
-            c0[r * 32 + lane] = t0;
-            if (KIND == kSumAndEnergy) {
-                c1[r * 32 + lane] = t1;
-                if (t1 != 0.0 && base + r * 32 + lane < nz) nz = base + r * 32 + lane;
+            for (int r = 0; r < kRows; ++r) {
+                const int i = r * 32 + lane;
+                const int64_t k = t * kTile + i;
+                const int64_t j = start + k - sig.head;
+                copy8(st + slot_of(i), sig.base + j, k < n && (uint64_t)j < (uint64_t)sig.avail);
             }
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");  // empty past the end: the count stays uniform
     };
-    if (n <= 0) return;
-    load(0);
-    store(0, 0);
-    __syncwarp();
-    int buf = 0;
-    for (int64_t base = 0; base < n; base += kTile) {
-        const int64_t next = base + kTile;
-        if (next < n) load(next);
-        const double *c0 = tiles + buf * 2 * kTile, *c1 = c0 + kTile;
-        const int64_t left = n - base;
-        if (left >= kTile) {
-            // addends two at a time (16-byte broadcast loads), in index order
-            const double2 *d0 = reinterpret_cast<const double2 *>(c0);
-            const double2 *d1 = reinterpret_cast<const double2 *>(c1);
-#pragma unroll 16
-            for (int e = 0; e < kTile / 2; ++e) {
-                const double2 a = d0[e];
-                acc0 += a.x;
-                acc0 += a.y;
-                if (KIND == kSumAndEnergy) {
-                    const double2 b = d1[e];
-                    acc1 += b.x;
-                    acc1 += b.y;
-                }
+#pragma unroll
+    for (int t = 0; t < kStages - 1; ++t) issue(t);
+    int64_t nz = n;
+    for (int64_t t = 0; t < ntiles; ++t) {
+        issue(t + kStages - 1);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 1) : "memory");
+        __syncwarp();
+        double *st = stages + (int)(t % kStages) * kSlots;
+        const int left = (int)(n - t * kTile < kTile ? n - t * kTile : kTile);
+        double own[kRows];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) own[j] = st[lane * kPad + j];
+        if (KIND == kSumAndEnergy) {
+            double sq[kRows];
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) sq[j] = own[j] * own[j];
+            if (nz == n) {
+                int f = kTile;
+#pragma unroll
+                for (int j = kRows - 1; j >= 0; --j)
+                    if (sq[j] != 0.0 && lane * kRows + j < left) f = lane * kRows + j;
+                f = __reduce_min_sync(0xffffffffu, f);
+                if (f < kTile) nz = t * kTile + f;
+            }
+            const int k0 = exact_prefix(acc0, own, left);
+            const int k1 = exact_prefix(acc1, sq, left);
+            for (int i = k0 < k1 ? k0 : k1; i < left; ++i) {
+                const double x = st[slot_of(i)];
+                if (i >= k0) acc0 += x;
+                if (i >= k1) acc1 += x * x;
+            }
+        } else if (KIND == kEnergy) {
+            double sq[kRows];
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) sq[j] = own[j] * own[j];
+            const int k0 = exact_prefix(acc0, sq, left);
+            if (k0 < left) {
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < kRows; ++j) st[lane * kPad + j] = sq[j];
+                __syncwarp();
+                serial_add(acc0, st, k0, left);
             }
         } else {
-            for (int e = 0; e < (int)left; ++e) {
-                acc0 += c0[e];
-                if (KIND == kSumAndEnergy) acc1 += c1[e];
+            const int64_t k0 = start + t * kTile + lane * kRows;
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < kRows; ++j) {
+                const double d = own[j] - mean;
+                st[lane * kPad + j] = ((k0 + j) & 1) ? -d : d;
             }
+            __syncwarp();
+            serial_add(acc0, st, 0, left);
         }
-        if (next < n) store(next, buf ^ 1);
         __syncwarp();
-        buf ^= 1;
     }
-    if (KIND == kSumAndEnergy && first_nz) {
-        for (int off = 16; off > 0; off >>= 1) {
-            const int64_t o = __shfl_down_sync(0xffffffffu, nz, off);
-            nz = o < nz ? o : nz;
-        }
-        *first_nz = nz;  // lane 0's value is the warp's
-    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (KIND == kSumAndEnergy && first_nz) *first_nz = nz;
 }
 
 template <int KIND>
 __global__ void __launch_bounds__(32 * kSerialWarps) serial_sum_kernel(const SumJob *__restrict__ jobs, int njobs) {
-    __shared__ __align__(16) double tiles[kSerialWarps][4 * kTile];
+    __shared__ __align__(16) double tiles[kSerialWarps][kStages * kSlots];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -157,7 +259,7 @@ struct AlignedEnergyArgs {
 
 __global__ void __launch_bounds__(32 * kSerialWarps) aligned_energy_kernel(const AlignedEnergyArgs *__restrict__ jobs,
                                                                             int njobs) {
-    __shared__ __align__(16) double tiles[kSerialWarps][4 * kTile];
+    __shared__ __align__(16) double tiles[kSerialWarps][kStages * kSlots];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -397,7 +499,7 @@ uint64_t &launch_counter() {
 
 void launch_envelope_stats(const SumJob *d_jobs, int njobs, cudaStream_t s) {
     if (njobs <= 0) return;
-    const int per_block = 4;
+    const int per_block = kSerialWarps;
     const int grid = (njobs + per_block - 1) / per_block;
     serial_sum_kernel<kSumAndEnergy><<<grid, 32 * per_block, 0, s>>>(d_jobs, njobs);
     serial_sum_kernel<kNyquist><<<grid, 32 * per_block, 0, s>>>(d_jobs, njobs);
@@ -406,14 +508,14 @@ void launch_envelope_stats(const SumJob *d_jobs, int njobs, cudaStream_t s) {
 
 void launch_energy(const SumJob *d_jobs, int njobs, cudaStream_t s) {
     if (njobs <= 0) return;
-    const int per_block = 4;
+    const int per_block = kSerialWarps;
     serial_sum_kernel<kEnergy><<<(njobs + per_block - 1) / per_block, 32 * per_block, 0, s>>>(d_jobs, njobs);
     launch_counter() += 1;
 }
 
 void launch_aligned_energy(const void *d_args, int njobs, cudaStream_t s) {
     if (njobs <= 0) return;
-    const int per_block = 4;
+    const int per_block = kSerialWarps;
     aligned_energy_kernel<<<(njobs + per_block - 1) / per_block, 32 * per_block, 0, s>>>(
         static_cast<const AlignedEnergyArgs *>(d_args), njobs);
     launch_counter() += 1;

@@ -109,6 +109,28 @@ int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t
     return lag_stage(a, la, b, lb, lag, false);
 }
 
+int visqol_b200_signal_sums(const double *x, size_t len, size_t skip, double *out) {
+    if ((!x && len) || !out || skip > len) return stage_fail(VISQOL_E_INVALID_ARGUMENT, "invalid argument");
+    return guarded([&] {
+        DBuf<double> dx(x, len), dout(8);
+        const int64_t n = (int64_t)len, k = (int64_t)skip;
+        const vqb::SumJob whole{vqb::VSig{dx.p, 0, n, n}, dout.p};
+        // x[skip..] as a window: sample(i) = x[i + skip]
+        const vqb::SumJob tail{vqb::VSig{dx.p, -k, n, n - k}, dout.p + 4};
+        DBuf<vqb::SumJob> dw(&whole, 1), dt(&tail, 1);
+        vqb::launch_envelope_stats(dw.p, 1, 0);
+        vqb::launch_energy(dt.p, 1, 0);
+        VQB_CUDA(cudaDeviceSynchronize());
+        double h[8];
+        dout.get(h, 8);
+        out[0] = h[0];
+        out[1] = h[1];
+        out[2] = h[2];
+        out[3] = h[3];
+        out[4] = h[6];
+    });
+}
+
 int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb, int64_t *lag) {
     return lag_stage(a, la, b, lb, lag, true);
 }

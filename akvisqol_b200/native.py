@@ -147,6 +147,7 @@ def _load() -> ctypes.CDLL:
         "visqol_b200_spectrogram": (c_int, [c_size_t, D, D, c_size_t, c_size_t, D, c_size_t, D, SZ]),
         "visqol_b200_envelope_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
         "visqol_b200_best_lag": (c_int, [D, c_size_t, D, c_size_t, I64]),
+        "visqol_b200_signal_sums": (c_int, [D, c_size_t, c_size_t, D]),
         "visqol_b200_lag_search": (c_int, [D, c_size_t, D, c_size_t, c_int, c_int, I64, POINTER(c_int32),
                                            POINTER(c_float), c_size_t]),
         "visqol_b200_refine_lag": (c_int, [D, c_size_t, D, c_size_t, POINTER(c_float), c_size_t, c_double, c_double,
@@ -200,6 +201,7 @@ EXPORTS = [
     "visqol_measure_batch", "visqol_measure_files_batch", "visqol_result_free",
     "visqol_b200_measure_batch", "visqol_b200_measure_batch_grad", "visqol_b200_trace_free", "visqol_b200_last_timing", "visqol_b200_device_info",
     "visqol_b200_spectrogram", "visqol_b200_envelope_lag", "visqol_b200_best_lag", "visqol_b200_fft",
+    "visqol_b200_signal_sums",
     "visqol_b200_lag_search", "visqol_b200_refine_lag", "visqol_b200_nsim_quotient",
     "visqol_b200_patch_similarity_grad", "visqol_b200_prepare_grad",
     "visqol_b200_prepare_for_comparison", "visqol_b200_log10", "visqol_b200_nsim_table", "visqol_b200_dp",
@@ -544,6 +546,17 @@ def envelope_lag(a, b) -> int:
     lag = c_int64()
     _check(lib.visqol_b200_envelope_lag(_dptr(a), a.size, _dptr(b), b.size, ctypes.byref(lag)))
     return lag.value
+
+
+def signal_sums(x, skip: int = 0) -> dict:
+    """The serial statistics of x as the CPU sums them, bit for bit:
+    {"sum", "nyquist", "energy", "first_nonzero", "aligned_energy"} (the
+    last over x[skip:]); see visqol_b200_signal_sums."""
+    x = mono(x, "x")
+    out = np.zeros(5)
+    _check(lib.visqol_b200_signal_sums(_dptr(x), x.size, skip, _dptr(out)))
+    return {"sum": out[0], "nyquist": out[1], "energy": out[2], "first_nonzero": int(out[3]),
+            "aligned_energy": out[4]}
 
 
 def best_lag(a, b) -> int:

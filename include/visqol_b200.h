@@ -226,6 +226,15 @@ int visqol_b200_spectrogram(size_t nb, const double *coeffs, const double *hann,
 int visqol_b200_envelope_lag(const double *a, size_t la, const double *b, size_t lb,
                              int64_t *lag);
 
+/* A signal's serial statistics, each in the CPU's left-to-right f64
+ * summation order, bit for bit: out[0] = sum x, out[1] = sum (-1)^k
+ * (x - out[0] / len) (upperEnvelope's Nyquist bin, reference
+ * src/envelope.zig:28-41), out[2] = sum x*x (reference src/audio.zig:132-136),
+ * out[3] = the first k with x[k]*x[k] != 0 (len if none), out[4] = sum x*x
+ * over x[skip..] (the energy of a lag-aligned signal, src/realign.zig:91-110).
+ * skip <= len. */
+int visqol_b200_signal_sums(const double *x, size_t len, size_t skip, double *out);
+
 /* Raw-signal FFT cross-correlation lag (reference src/xcorr.zig:197-251). */
 int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb,
                          int64_t *lag);
