@@ -311,7 +311,7 @@ int32_t *Engine::launch_lag_jobs(std::vector<LagJob> &jobs, bool raw, bool exact
     std::map<int64_t, std::vector<size_t>> groups;
     for (size_t i = 0; i < jobs.size(); ++i) groups[jobs[i].n].push_back(i);
     const size_t budget = size_t(4) << 30;
-    const bool f32 = opt_.form == kFormF32 && !exact;
+    const bool f32 = !exact && !opt_.exact_lag_search;
     int32_t *d_status = nullptr;
     if (f32) {
         d_status = arena_.alloc_n<int32_t>(jobs.size());
@@ -972,7 +972,7 @@ void Engine::measure_batch(size_t n, const double *const *refs, const size_t *re
                 lag_jobs.push_back(j);
                 lag_pair.push_back(i);
                 s.trace.fft_nlogn += 2.0 * (double)j.n * std::log2((double)j.n);
-                timing_.lag_bytes += lag_search_bytes(j, opt_.form == kFormF32);
+                timing_.lag_bytes += lag_search_bytes(j, !opt_.exact_lag_search);
             }
         }
         launch_sums(sums);

@@ -30,6 +30,11 @@ struct Options {
     bool disable_realignment = false;
     // Arithmetic form (kFormExact, kFormF32, kFormF64).
     int32_t form = kFormExact;
+    // Lag searches by the f64 transform throughout. Otherwise (every form)
+    // the f32 transform nominates the near-maxima, f64 dot products rescore
+    // them, and the searches that leaves undecided (near-ties, more than
+    // kLagCandCap candidates) rerun with the f64 transform: the same lags.
+    bool exact_lag_search = false;
 };
 
 struct PairTrace {

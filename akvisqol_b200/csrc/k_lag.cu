@@ -784,7 +784,7 @@ __device__ inline void cp_async8z(double *dst, const double *src, bool in) {
 // form's loads queue behind its 128-register budget. The values, and so the
 // results, are the register form's. The stage is then the exchange buffer.
 template <class C, int G, bool RAW>
-__global__ void __launch_bounds__(kThreads, 2) fwd_columns_staged(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, sizeof(C) == 8 ? 3 : 2) fwd_columns_staged(const LagJob *__restrict__ jobs,
                                                                const C *__restrict__ tcol) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *sm = reinterpret_cast<C *>(smem_raw);
@@ -1053,7 +1053,7 @@ __global__ void __launch_bounds__(kThreads) inv_columns_nominate(const LagJob *_
 
 // Pass 3 of the f32 search, register form (4 <= G <= 11).
 template <int G>
-__global__ void __launch_bounds__(kThreads, 2) inv_columns_reg_nominate(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, 3) inv_columns_reg_nominate(const LagJob *__restrict__ jobs,
                                                                      const float2 *__restrict__ tcol, int parts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *sm = reinterpret_cast<float2 *>(smem_raw);
@@ -1208,19 +1208,28 @@ __global__ void __launch_bounds__(kThreads) pick_candidates(const LagJob *__rest
 }
 
 constexpr int kRescoreChunk = 4096;  // b samples per rescoring CTA
+constexpr int kRescoreSpan = 1024;   // widest candidate lag range staged with a chunk
 
 // Partial dot products sum_j a[j + lag] b[j] of every candidate lag over
 // this CTA's chunk of b (reference dotAtLag src/xcorr.zig:328-340; the
 // summation order is this kernel's, fixed), of the envelopes (or raw
-// signals), in f64. Up to kRescoreGroup candidates (usually neighbouring
-// lags) share one pass over the chunk: b's value is formed once, a's for
-// each lag hit the same cache lines. grid (chunks, jobs).
-constexpr int kRescoreGroup = 8;
+// signals), in f64: each thread adds its 16 products in order, the warps
+// reduce by shuffles and the 8 warp sums are added in order. When the
+// candidates lie within kRescoreSpan lags of each other (near-maxima of one
+// peak, the usual case) the envelope of a over the chunk's window and of b
+// over the chunk are formed once, into shared memory and registers, and
+// every candidate reads them; otherwise each candidate takes its own pass,
+// forming the values it needs. grid (chunks, jobs).
 template <bool RAW>
 __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__restrict__ jobs, int nchunks) {
+    __shared__ double win[kRescoreChunk + kRescoreSpan];
+    __shared__ double part[kLagCandCap][kThreads / 32];
+    __shared__ int32_t keys[kLagCandCap];
+    constexpr int kPer = kRescoreChunk / kThreads;
     const LagJob job = jobs[blockIdx.y];
     if (*job.status != 0) return;
     const int count = *job.ncand;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     EnvParams pa{}, pb{};
     if (!RAW) {
         pa = env_params(job.a, job.stats_a);
@@ -1228,33 +1237,62 @@ __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__r
     }
     const int64_t max_lag = job.biggest - 1;
     const int64_t j0 = (int64_t)blockIdx.x * kRescoreChunk;
-    for (int c0 = 0; c0 < count; c0 += kRescoreGroup) {
-        const int cn = count - c0 < kRescoreGroup ? count - c0 : kRescoreGroup;
-        int64_t lag[kRescoreGroup];
-        double acc[kRescoreGroup];
-#pragma unroll
-        for (int g = 0; g < kRescoreGroup; ++g) {
-            lag[g] = g < cn ? (int64_t)job.cand_key[c0 + g] - max_lag : 0;
-            acc[g] = 0.0;
+    if (threadIdx.x < count) keys[threadIdx.x] = job.cand_key[threadIdx.x];
+    __syncthreads();
+    int kmin = INT32_MAX, kmax = INT32_MIN;
+    for (int c = 0; c < count; ++c) {
+        kmin = min(kmin, keys[c]);
+        kmax = max(kmax, keys[c]);
+    }
+    // a warp's 32 partial sums, in lane order by halves, into lane 0
+    auto warp_sum = [](double v) {
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        return v;
+    };
+    if (count > 0 && kmax - kmin <= kRescoreSpan) {
+        const int64_t ws = j0 + (int64_t)kmin - max_lag;  // a index of win[0]
+        const int wlen = kRescoreChunk + (kmax - kmin);
+        for (int e = threadIdx.x; e < wlen; e += kThreads) {
+            const int64_t ia = ws + e;
+            win[e] = ia >= 0 && ia < job.a.len ? (RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia)) : 0.0;
         }
-#pragma unroll 2
-        for (int k = 0; k < kRescoreChunk / kThreads; ++k) {
-            const int64_t j = j0 + threadIdx.x + k * kThreads;
-            if (j >= job.b.len) continue;
-            const double y = RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j);
+        double y[kPer];
 #pragma unroll
-            for (int g = 0; g < kRescoreGroup; ++g) {
-                const int64_t ia = j + lag[g];
-                if (g < cn && ia >= 0 && ia < job.a.len) {
+        for (int k = 0; k < kPer; ++k) {
+            const int64_t j = j0 + threadIdx.x + k * kThreads;
+            y[k] = j < job.b.len ? (RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j)) : 0.0;
+        }
+        __syncthreads();
+        for (int c = 0; c < count; ++c) {
+            const double *w = win + (keys[c] - kmin) + threadIdx.x;
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) acc += w[k * kThreads] * y[k];
+            acc = warp_sum(acc);
+            if (lane == 0) part[c][warp] = acc;
+        }
+    } else {
+        for (int c = 0; c < count; ++c) {
+            const int64_t lag = (int64_t)keys[c] - max_lag;
+            double acc = 0.0;
+            for (int k = 0; k < kPer; ++k) {
+                const int64_t j = j0 + threadIdx.x + k * kThreads, ia = j + lag;
+                if (j < job.b.len && ia >= 0 && ia < job.a.len) {
+                    const double y = RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j);
                     const double x = RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia);
-                    acc[g] += x * y;
+                    acc += x * y;
                 }
             }
+            acc = warp_sum(acc);
+            if (lane == 0) part[c][warp] = acc;
         }
-        for (int g = 0; g < cn; ++g) {
-            const double t = block_sum(acc[g]);
-            if (threadIdx.x == 0) job.rescore[(int64_t)(c0 + g) * nchunks + blockIdx.x] = t;
-        }
+    }
+    __syncthreads();
+    if (threadIdx.x < count) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; ++w) t += part[threadIdx.x][w];
+        job.rescore[(int64_t)threadIdx.x * nchunks + blockIdx.x] = t;
     }
 }
 

@@ -23,20 +23,20 @@ enum SumKind : int {
     kEnergy = 2,        // out[2] = sum x*x
 };
 
-// Tiles of 256 consecutive samples move into this warp's shared-memory
-// stages by asynchronous copies (each lane 8 samples of coalesced 256-byte
-// rows; zeros outside the stored window), kStages tiles in flight. In a
-// stage, the 8 samples k = 8L .. 8L+7 of the tile sit at L * kPad + (k & 7):
-// lane L reads its own run without bank conflicts, and all lanes read any
-// one sample as a broadcast.
-constexpr int kRows = 8;
+// Tiles of 1024 consecutive samples move into this warp's shared-memory
+// stages by asynchronous copies (coalesced 256-byte rows; zeros outside the
+// stored window), kStages tiles in flight. In a stage, the 32 samples
+// k = 32L .. 32L+31 of the tile sit at L * kPad + (k & 31): lane L reads its
+// own run without bank conflicts, and all lanes read any one sample as a
+// broadcast.
+constexpr int kRows = 32;
 constexpr int kTile = 32 * kRows;
 constexpr int kPad = kRows + 1;
 constexpr int kSlots = 32 * kPad;
-constexpr int kStages = 8;
-constexpr int kSerialWarps = 2;
+constexpr int kStages = 4;
+constexpr int kSerialWarps = 1;
 
-__device__ inline int slot_of(int i) { return (i >> 3) * kPad + (i & 7); }
+__device__ inline int slot_of(int i) { return (i >> 5) * kPad + (i & 31); }
 
 __device__ double g_copy_guard;  // source address of the zero-filling copies
 
@@ -52,165 +52,250 @@ __device__ inline void copy8(double *dst, const double *src, bool in) {
 // While the running sum stays in one binade [2^e, 2^(e+1)), every value it
 // takes is a multiple of u = 2^(e-52), and s + t rounds to the multiple of u
 // nearest the exact value, s + u * rint(t / u), unless t / u is a
-// half-integer (a tie, which round-half-even settles by the parity of s). A
-// tile of terms is then added as integers: q = rint(t / u) per term, a
-// prefix sum over the warp, and a check that every partial sum M (in units
-// of u) stays a unit inside the binade, 2^52 + 1 <= M <= 2^53 - 2, so that
-// the exact value of each addition, within half a unit of u * M, lies in the
-// binade as well. The first term that breaks a condition ends the shortcut:
-// the sum before it is exact, and the caller adds the rest one at a time.
-// t: this lane's terms (tile index 8 * lane + j); left: the tile's terms.
-// Returns how many leading terms were added into s (the same in all lanes).
-__device__ inline int exact_prefix(double &s, const double (&t)[kRows], int left) {
-    const int lane = threadIdx.x & 31;
-    const long long bits = __double_as_longlong(s);
-    const int e = (int)((bits >> 52) & 0x7ff);
-    // zero, subnormal or below 2^-970 (the unit scales below must be
-    // normal), infinite or NaN: no shortcut
-    if (e < 53 || e == 0x7ff) return 0;
-    const double to_units = __longlong_as_double((long long)(2098 - e) << 52);  // 1 / u
-    const double from_units = __longlong_as_double((long long)(e - 52) << 52);  // u
-    const bool neg = bits < 0;
-    long long run[kRows];
-    long long acc = 0;
-    unsigned ok = 0;
-#pragma unroll
-    for (int j = 0; j < kRows; ++j) {
-        // a power-of-two scale is exact (a result far below 1/2 may round,
-        // but rounds to q = 0 either way)
-        const double tau = neg ? -(t[j] * to_units) : t[j] * to_units;
+// half-integer (a tie, which round-half-even settles by the parity of s).
+// A tile of terms then adds as integers in units of u: q = rint(t / u) per
+// term, a prefix sum over the warp, and a check that every partial sum M
+// stays a unit inside the binade, 2^52 + 1 <= M <= 2^53 - 2, so that the
+// exact value of each addition, within half a unit of u * M, lies in the
+// binade as well. The integers are held in f64. Every lane runs a sum of
+// its own q and the warp scans the lane totals; the checks find the first
+// lane holding a failing position exactly: before it, every partial sum
+// (a difference of two valid M) is an integer below 2^52 in magnitude; in
+// it, each of its sums up to the failing position adds one |q| <= 2^52 to
+// such a sum, which stays below 2^53; and its starting offset comes from the
+// exclusive scan of the lanes before it alone. The lanes before it are
+// added at once, that lane's run one term at a time, and the rest of the
+// tile is tried again from the new sum.
+constexpr double kLo = 0x1p52 + 1.0, kHi = 0x1p53 - 2.0;
+constexpr int kMinRetry = 96;  // fewer terms left in a tile than this are added one at a time
+constexpr int kMaxRetries = 3;  // shortcut attempts after the first in one tile
+
+struct Chain {
+    double to, from, m0;  // +-1/u, +-u (the sum's sign folded in), |s| / u
+    bool ok;              // s is normal and above 2^-970 (the unit scales are normal)
+    double run, lo, hi;   // this lane's running sum of q, and its extremes over its positions
+    bool good;            // no tie or oversized term among this lane's positions
+    __device__ inline void begin(double s) {
+        const long long bits = __double_as_longlong(s);
+        const int e = (int)((bits >> 52) & 0x7ff);
+        ok = e >= 53 && e != 0x7ff;
+        const double inv = __longlong_as_double((long long)((unsigned long long)(2098 - e) << 52));
+        const double u = __longlong_as_double((long long)((unsigned long long)(e - 52) << 52));
+        to = bits < 0 ? -inv : inv;
+        from = bits < 0 ? -u : u;
+        m0 = (double)((bits & ((1LL << 52) - 1)) | (1LL << 52));
+        run = 0.0;
+        lo = INFINITY;
+        hi = -INFINITY;
+        good = true;
+    }
+    // the term t of this lane's next position (a zero-filled position past
+    // the end adds q = 0)
+    __device__ inline void add(double t) {
+        const double tau = t * to;  // a power-of-two scale: exact (or far below 1/2)
         const double q = rint(tau);
-        const bool good = fabs(q) <= 0x1p53 && fabs(tau - q) != 0.5;  // NaN and inf fail the first test
-        acc += good ? (long long)q : 0;
-        run[j] = acc;
-        ok |= (unsigned)good << j;
+        // |q| <= 2^52 keeps every partial sum up to the first failing position
+        // below 2^53 (exact); NaN and inf fail the first test
+        const bool b = fabs(q) <= 0x1p52 && fabs(tau - q) != 0.5;
+        good = good && b;
+        run += b ? q : 0.0;
+        lo = run < lo ? run : lo;
+        hi = run > hi ? run : hi;
     }
-    long long incl = acc;
+    // After the lanes' passes: adds to s every lane before the first lane
+    // holding a failing position, or the whole tile; returns that lane (32
+    // if none). The same in all lanes.
+    __device__ inline int settle(double &s) const {
+        const int lane = threadIdx.x & 31;
+        double incl = run;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const long long v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        const double base = m0 + (lane == 0 ? 0.0 : excl);
+        const unsigned failing = __ballot_sync(0xffffffffu, !(good && base + lo >= kLo && base + hi <= kHi));
+        const int fail = failing ? __ffs(failing) - 1 : 32;
+        // every lane before the first failing one holds only valid partial
+        // sums, so the sum at the start of that lane's run is exact
+        s = (fail < 32 ? __shfl_sync(0xffffffffu, base, fail & 31) : m0 + __shfl_sync(0xffffffffu, incl, 31)) * from;
+        return fail;
     }
-    const long long base = ((bits & ((1LL << 52) - 1)) | (1LL << 52)) + (incl - acc);
-    int first = kTile;
-#pragma unroll
-    for (int j = kRows - 1; j >= 0; --j) {
-        const long long m = base + run[j];
-        const bool bad = !((ok >> j) & 1u) || m < (1LL << 52) + 1 || m > (1LL << 53) - 2;
-        if (bad && lane * kRows + j < left) first = lane * kRows + j;
-    }
-    int k = __reduce_min_sync(0xffffffffu, first);
-    k = k < left ? k : left;
-    if (k > 0) {
-        const int last = k - 1, js = last & (kRows - 1);
-        long long mine = 0;
-#pragma unroll
-        for (int j = 0; j < kRows; ++j)
-            if (j == js) mine = base + run[j];
-        const long long m = __shfl_sync(0xffffffffu, mine, last >> 3);
-        const double v = (double)m * from_units;  // m < 2^53: exact
-        s = neg ? -v : v;
-    }
-    return k;
+};
+
+// True when every term of the tile from position k on is zero: a sum at +0
+// stays +0 through them.
+__device__ inline bool zeros_from(const double *own, int k) {
+    const int lane = threadIdx.x & 31;
+    bool z = true;
+#pragma unroll 8
+    for (int j = 0; j < kRows; ++j) z = z && (lane * kRows + j < k || own[j] == 0.0);
+    return __all_sync(0xffffffffu, z);
 }
 
-// acc += stage terms from .. to - 1, in index order (every lane the same).
-__device__ inline void serial_add(double &acc, const double *st, int from, int to) {
-    if (from == 0 && to == kTile) {
-#pragma unroll 8
-        for (int g = 0; g < 32; ++g) {
-            const double *p = st + g * kPad;
-            double v[kRows];
+// s += the tile's terms of one chain at positions from .. to - 1 (all in one
+// lane's run of 32), one at a time in index order. Positions outside the
+// range add +0.0, which leaves any sum that started at +0.0 unchanged (such
+// a sum is never -0.0).
+template <bool SQUARE>
+__device__ inline void serial_run(double &s, const double *st, int run_start, int from, int to) {
+    const double *p = st + (run_start >> 5) * kPad;
+    double v[kRows];
 #pragma unroll
-            for (int j = 0; j < kRows; ++j) v[j] = p[j];
-#pragma unroll
-            for (int j = 0; j < kRows; ++j) acc += v[j];
-        }
-    } else {
-#pragma unroll 8
-        for (int i = from; i < to; ++i) acc += st[slot_of(i)];
+    for (int j = 0; j < kRows; ++j) {
+        const int i = run_start + j;
+        const double x = p[j];
+        v[j] = i >= from && i < to ? (SQUARE ? x * x : x) : 0.0;
     }
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) s += v[j];
+}
+
+// The rest of a tile from position k, where the shortcut stopped: the run
+// holding k one term at a time, then the shortcut again over what follows
+// (at most kMaxRetries times), else term by term to the end.
+template <bool SQUARE>
+__device__ __noinline__ void add_rest(double &s, const double *st, const double *own, int k, int left) {
+    const int lane = threadIdx.x & 31;
+    for (int tries = 0;; ++tries) {
+        const int end = (k | (kRows - 1)) + 1 < left ? (k | (kRows - 1)) + 1 : left;
+        serial_run<SQUARE>(s, st, k & ~(kRows - 1), k, end);
+        k = end;
+        if (k >= left) return;
+        if (left - k < kMinRetry || tries == kMaxRetries) break;
+        if (s == 0.0 && zeros_from(own, k)) return;
+        Chain c;
+        c.begin(s);
+        if (!c.ok) continue;
+#pragma unroll 8
+        for (int j = 0; j < kRows; ++j) c.add(lane * kRows + j >= k ? (SQUARE ? own[j] * own[j] : own[j]) : 0.0);
+        // Lanes wholly before k add only zeros: settle leaves s as it was if
+        // one of them is reported (its check sees s itself, which may sit
+        // on the binade's edge), and k does not move back.
+        const int fail = c.settle(s);
+        if (fail == 32) return;
+        k = fail * kRows > k ? fail * kRows : k;
+    }
+    for (; k < left; k = (k & ~(kRows - 1)) + kRows) serial_run<SQUARE>(s, st, k & ~(kRows - 1), k, left);
+}
+
+// One chain's tile after its pass: the shortcut where the checks pass, the
+// rest through add_rest.
+template <bool SQUARE>
+__device__ inline void finish_tile(double &s, const Chain &c, const double *st, const double *own, int left) {
+    if (s == 0.0 && zeros_from(own, 0)) return;
+    int k = 0;
+    if (c.ok) {
+        const int fail = c.settle(s);
+        if (fail == 32) return;
+        k = fail * kRows;
+    }
+    add_rest<SQUARE>(s, st, own, k, left);
 }
 
 // Left-to-right sums, in index order, of KIND's per-sample terms over
 // sample(start + k), k in [0, n): chain 0 (and chain 1 for kSumAndEnergy).
-// Sums of x and x*x take the exact integer shortcut tile by tile; the
-// alternating Nyquist sum, whose running value changes binade every few
-// samples, is added one term at a time from the staged terms.
-// stages: this warp's kStages * kSlots doubles. first_nz (kSumAndEnergy):
-// the first k whose x*x is nonzero, n if none.
+// Sums of x and x*x take the exact integer shortcut tile by tile and add
+// term by term where it does not apply; the alternating Nyquist sum, whose
+// running value changes binade every few samples, is added term by term
+// from staged terms. stages: this warp's kStages * kSlots doubles.
+// first_nz (kSumAndEnergy): the first k whose x*x is nonzero, n if none.
 template <int KIND>
 __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, double mean, double &acc0,
                                    double &acc1, double *stages, int64_t *first_nz = nullptr) {
     const int lane = threadIdx.x & 31;
     if (n <= 0) return;
     const int64_t ntiles = (n + kTile - 1) / kTile;
-    auto issue = [&](int64_t t) {
+    auto issue_row = [&](int64_t t, int r) {  // row r of tile t (32 samples), if the tile exists
         if (t < ntiles) {
-            double *st = stages + (int)(t % kStages) * kSlots;
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int i = r * 32 + lane;
-                const int64_t k = t * kTile + i;
-                const int64_t j = start + k - sig.head;
-                copy8(st + slot_of(i), sig.base + j, k < n && (uint64_t)j < (uint64_t)sig.avail);
-            }
+            const int64_t k = t * kTile + r * 32 + lane;
+            const int64_t j = start + k - sig.head;
+            copy8(stages + (int)(t % kStages) * kSlots + r * kPad + lane, sig.base + j,
+                  k < n && (uint64_t)j < (uint64_t)sig.avail);
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");  // empty past the end: the count stays uniform
+    };
+    auto commit = [] { asm volatile("cp.async.commit_group;\n" ::: "memory"); };  // one group a tile, even empty
+    auto issue = [&](int64_t t) {
+#pragma unroll 8
+        for (int r = 0; r < kRows; ++r) issue_row(t, r);
+        commit();
     };
 #pragma unroll
     for (int t = 0; t < kStages - 1; ++t) issue(t);
     int64_t nz = n;
     for (int64_t t = 0; t < ntiles; ++t) {
-        issue(t + kStages - 1);
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 1) : "memory");
+        if (KIND == kNyquist) {
+            // the next tile's copies are issued among this tile's additions
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+        } else {
+            issue(t + kStages - 1);
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 1) : "memory");
+        }
         __syncwarp();
         double *st = stages + (int)(t % kStages) * kSlots;
+        double *own = st + lane * kPad;
         const int left = (int)(n - t * kTile < kTile ? n - t * kTile : kTile);
-        double own[kRows];
-#pragma unroll
-        for (int j = 0; j < kRows; ++j) own[j] = st[lane * kPad + j];
         if (KIND == kSumAndEnergy) {
-            double sq[kRows];
-#pragma unroll
-            for (int j = 0; j < kRows; ++j) sq[j] = own[j] * own[j];
+            Chain c0, c1;
+            c0.begin(acc0);
+            c1.begin(acc1);
+#pragma unroll 8
+            for (int j = 0; j < kRows; ++j) {
+                const double x = own[j];
+                c0.add(x);
+                c1.add(x * x);
+            }
             if (nz == n) {
                 int f = kTile;
-#pragma unroll
                 for (int j = kRows - 1; j >= 0; --j)
-                    if (sq[j] != 0.0 && lane * kRows + j < left) f = lane * kRows + j;
+                    if (own[j] * own[j] != 0.0) f = lane * kRows + j;
                 f = __reduce_min_sync(0xffffffffu, f);
-                if (f < kTile) nz = t * kTile + f;
+                if (f < left) nz = t * kTile + f;
             }
-            const int k0 = exact_prefix(acc0, own, left);
-            const int k1 = exact_prefix(acc1, sq, left);
-            for (int i = k0 < k1 ? k0 : k1; i < left; ++i) {
-                const double x = st[slot_of(i)];
-                if (i >= k0) acc0 += x;
-                if (i >= k1) acc1 += x * x;
-            }
+            finish_tile<false>(acc0, c0, st, own, left);
+            finish_tile<true>(acc1, c1, st, own, left);
         } else if (KIND == kEnergy) {
-            double sq[kRows];
-#pragma unroll
-            for (int j = 0; j < kRows; ++j) sq[j] = own[j] * own[j];
-            const int k0 = exact_prefix(acc0, sq, left);
-            if (k0 < left) {
-                __syncwarp();
-#pragma unroll
-                for (int j = 0; j < kRows; ++j) st[lane * kPad + j] = sq[j];
-                __syncwarp();
-                serial_add(acc0, st, k0, left);
-            }
+            Chain c0;
+            c0.begin(acc0);
+#pragma unroll 8
+            for (int j = 0; j < kRows; ++j) c0.add(own[j] * own[j]);
+            finish_tile<true>(acc0, c0, st, own, left);
         } else {
             const int64_t k0 = start + t * kTile + lane * kRows;
-            __syncwarp();
-#pragma unroll
+#pragma unroll 8
             for (int j = 0; j < kRows; ++j) {
                 const double d = own[j] - mean;
-                st[lane * kPad + j] = ((k0 + j) & 1) ? -d : d;
+                own[j] = ((k0 + j) & 1) ? -d : d;
             }
             __syncwarp();
-            serial_add(acc0, st, 0, left);
+            const int64_t next = t + kStages - 1;
+            if (left == kTile) {
+                // one run's loads in flight while the previous run is added
+                double v[kRows], w[kRows];
+#pragma unroll
+                for (int j = 0; j < kRows; ++j) v[j] = st[j];
+#pragma unroll
+                for (int g = 0; g < 32; g += 2) {
+                    issue_row(next, g);
+#pragma unroll
+                    for (int j = 0; j < kRows; ++j) w[j] = st[(g + 1) * kPad + j];
+#pragma unroll
+                    for (int j = 0; j < kRows; ++j) acc0 += v[j];
+                    issue_row(next, g + 1);
+                    if (g + 2 < 32) {
+#pragma unroll
+                        for (int j = 0; j < kRows; ++j) v[j] = st[(g + 2) * kPad + j];
+                    }
+#pragma unroll
+                    for (int j = 0; j < kRows; ++j) acc0 += w[j];
+                }
+            } else {
+#pragma unroll 8
+                for (int r = 0; r < kRows; ++r) issue_row(next, r);
+                for (int i = 0; i < left; ++i) acc0 += st[slot_of(i)];
+            }
+            commit();
         }
         __syncwarp();
     }

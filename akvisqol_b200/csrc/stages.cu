@@ -54,6 +54,7 @@ vqb::Engine &stage_engine(int form = vqb::kFormExact) {
         cudaGetDevice(&dev);
         vqb::Options o;
         o.form = form;
+        o.exact_lag_search = form == vqb::kFormExact;  // the stage lag calls' exact search
         e[form] = std::make_unique<vqb::Engine>(dev, o, nullptr);
     }
     return *e[form];

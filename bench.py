@@ -45,7 +45,9 @@ METRICS = {
     "exact": "ViSQOL pairs/s (audio mode, 10 s 48 kHz pairs), exact FP64 form, 1 B200",
 }
 DTYPES = {"fast": "f32 (gammatone stages 3-4 above the lowest band group, lag-search transform; rescoring, "
-                  "NSIM, DP, MOS in f64)", "balanced": "f64 (FMA)", "exact": "f64"}
+                  "NSIM, DP, MOS in f64)",
+          "balanced": "f64 (FMA); the lag search's nominating transform in f32, its rescoring in f64",
+          "exact": "f64; the lag search's nominating transform in f32, its rescoring in f64"}
 # gammatone: pipe-peak kind of visqol_b200_peak and the algorithm's flops per
 # sample, the same for every form: 4 biquads of 7 flops, the window multiply
 # and the square-accumulate (reference src/gammatone.zig:268-306)
