@@ -452,9 +452,38 @@ constexpr int kPadB = kB + kB / 16;
 
 __device__ inline int padi(int e) { return e + (e >> 4); }
 
+// x W_16^k, or x conj(W_16^k) (CONJ), W_16^k = e^{-2 pi i k / 16}, k < 8:
+// the f32 search's span-16 stages take their twiddles as constants, the
+// products by 1 and -i as exchanges and the ones by W_16^2 and W_16^6 as a
+// sum and a difference scaled once. k is a constant once the stage loops
+// are unrolled, so the switch folds.
+__device__ inline float2 w16_mul(float2 x, int k, bool conj) {
+    constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508978f, h = 0.70710678118654752f;
+    float wr = 1.0f, wi = 0.0f;
+    switch (k) {
+        case 0:
+            return x;
+        case 2:
+            return conj ? make_float2(h * (x.x - x.y), h * (x.x + x.y)) : make_float2(h * (x.x + x.y), h * (x.y - x.x));
+        case 4:
+            return conj ? make_float2(-x.y, x.x) : make_float2(x.y, -x.x);
+        case 6:
+            return conj ? make_float2(-h * (x.x + x.y), h * (x.x - x.y))
+                        : make_float2(h * (x.y - x.x), -h * (x.x + x.y));
+        case 1: wr = c1, wi = -s1; break;
+        case 3: wr = s1, wi = -c1; break;
+        case 5: wr = -s1, wi = -c1; break;
+        default: wr = -c1, wi = -s1; break;
+    }
+    if (conj) wi = -wi;
+    return make_float2(__fmaf_rn(x.x, wr, -(x.y * wi)), __fmaf_rn(x.x, wi, x.y * wr));
+}
+
 template <class C, int S0>
 __device__ inline void dif16(C (&x)[16], int j, const C *__restrict__ tst) {
     constexpr int q = S0 / 16;
+    // spans 16 .. 2 (j = 0) of the f32 search: constant twiddles
+    constexpr bool konst = S0 == 16 && std::is_same<C, float2>::value;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int half = 8 >> r;
@@ -462,10 +491,14 @@ __device__ inline void dif16(C (&x)[16], int j, const C *__restrict__ tst) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const C w = __ldg(tw + j + (m & (half - 1)) * q);
             const C a = x[m], b = x[m + half];
             x[m] = cadd(a, b);
-            x[m + half] = cmul(csub(a, b), w);
+            if constexpr (konst) {
+                x[m + half] = w16_mul(csub(a, b), (m & (half - 1)) << r, false);
+            } else {
+                const C w = __ldg(tw + j + (m & (half - 1)) * q);
+                x[m + half] = cmul(csub(a, b), w);
+            }
         }
     }
 }
@@ -473,6 +506,7 @@ __device__ inline void dif16(C (&x)[16], int j, const C *__restrict__ tst) {
 template <class C, int S0>
 __device__ inline void dit16(C (&x)[16], int j, const C *__restrict__ tst) {
     constexpr int q = S0 / 16;
+    constexpr bool konst = S0 == 16 && std::is_same<C, float2>::value;
 #pragma unroll
     for (int r = 3; r >= 0; --r) {
         const int half = 8 >> r;
@@ -480,8 +514,14 @@ __device__ inline void dit16(C (&x)[16], int j, const C *__restrict__ tst) {
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             if (m & half) continue;
-            const C w = __ldg(tw + j + (m & (half - 1)) * q);
-            const C a = x[m], b = cmul_conj(x[m + half], w);
+            C b;
+            if constexpr (konst) {
+                b = w16_mul(x[m + half], (m & (half - 1)) << r, true);
+            } else {
+                const C w = __ldg(tw + j + (m & (half - 1)) * q);
+                b = cmul_conj(x[m + half], w);
+            }
+            const C a = x[m];
             x[m] = cadd(a, b);
             x[m + half] = csub(a, b);
         }
@@ -1252,15 +1292,36 @@ __global__ void __launch_bounds__(kThreads) rescore_candidates(const LagJob *__r
     if (count > 0 && kmax - kmin <= kRescoreSpan) {
         const int64_t ws = j0 + (int64_t)kmin - max_lag;  // a index of win[0]
         const int wlen = kRescoreChunk + (kmax - kmin);
+        // a's stored samples over the window by asynchronous copies (all in
+        // flight at once, zeros outside them), b's by plain loads meanwhile
+        const double *guard = job.rescore;
         for (int e = threadIdx.x; e < wlen; e += kThreads) {
-            const int64_t ia = ws + e;
-            win[e] = ia >= 0 && ia < job.a.len ? (RAW ? vsig_at(job.a, ia) : env_at(job.a, pa, ia)) : 0.0;
+            const int64_t ia = ws + e, ja = ia - job.a.head;
+            const bool in = ia >= 0 && ia < job.a.len && (uint64_t)ja < (uint64_t)job.a.avail;
+            cp_async8z(win + e, in ? job.a.base + ja : guard, in);
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
         double y[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             const int64_t j = j0 + threadIdx.x + k * kThreads;
-            y[k] = j < job.b.len ? (RAW ? vsig_at(job.b, j) : env_at(job.b, pb, j)) : 0.0;
+            y[k] = j < job.b.len ? vsig_at(job.b, j) : 0.0;
+        }
+        if (!RAW) {
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const int64_t j = j0 + threadIdx.x + k * kThreads;
+                if (j < job.b.len) y[k] = env_of(y[k], pb, j);
+            }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        // each thread forms the envelope of the window entries it copied
+        for (int e = threadIdx.x; e < wlen; e += kThreads) {
+            const int64_t ia = ws + e;
+            if (ia < 0 || ia >= job.a.len)
+                win[e] = 0.0;
+            else if (!RAW)
+                win[e] = env_of(win[e], pa, ia);
         }
         __syncthreads();
         for (int c = 0; c < count; ++c) {

@@ -225,13 +225,8 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
     for (int t = 0; t < kStages - 1; ++t) issue(t);
     int64_t nz = n;
     for (int64_t t = 0; t < ntiles; ++t) {
-        if (KIND == kNyquist) {
-            // the next tile's copies are issued among this tile's additions
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
-        } else {
-            issue(t + kStages - 1);
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 1) : "memory");
-        }
+        issue(t + kStages - 1);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 1) : "memory");
         __syncwarp();
         double *st = stages + (int)(t % kStages) * kSlots;
         double *own = st + lane * kPad;
@@ -269,33 +264,19 @@ __device__ inline void warp_serial(const VSig &sig, int64_t start, int64_t n, do
                 own[j] = ((k0 + j) & 1) ? -d : d;
             }
             __syncwarp();
-            const int64_t next = t + kStages - 1;
             if (left == kTile) {
-                // one run's loads in flight while the previous run is added
-                double v[kRows], w[kRows];
+#pragma unroll 2
+                for (int g = 0; g < 32; ++g) {
+                    const double *p = st + g * kPad;
+                    double v[kRows];
 #pragma unroll
-                for (int j = 0; j < kRows; ++j) v[j] = st[j];
-#pragma unroll
-                for (int g = 0; g < 32; g += 2) {
-                    issue_row(next, g);
-#pragma unroll
-                    for (int j = 0; j < kRows; ++j) w[j] = st[(g + 1) * kPad + j];
+                    for (int j = 0; j < kRows; ++j) v[j] = p[j];
 #pragma unroll
                     for (int j = 0; j < kRows; ++j) acc0 += v[j];
-                    issue_row(next, g + 1);
-                    if (g + 2 < 32) {
-#pragma unroll
-                        for (int j = 0; j < kRows; ++j) v[j] = st[(g + 2) * kPad + j];
-                    }
-#pragma unroll
-                    for (int j = 0; j < kRows; ++j) acc0 += w[j];
                 }
             } else {
-#pragma unroll 8
-                for (int r = 0; r < kRows; ++r) issue_row(next, r);
                 for (int i = 0; i < left; ++i) acc0 += st[slot_of(i)];
             }
-            commit();
         }
         __syncwarp();
     }
