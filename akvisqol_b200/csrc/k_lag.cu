@@ -856,14 +856,35 @@ __global__ void __launch_bounds__(kThreads, sizeof(C) == 8 ? 3 : 2) fwd_columns_
     __syncthreads();
     C x[16];
     double ea = 0.0, eb = 0.0;
+    if constexpr (std::is_same<C, float2>::value && !RAW) {
+        // The f32 search forms the envelopes in f32: a few f32 ulps of each
+        // value, |delta corr| <= ~3 eps_f32 (|a|^2 + |b|^2), far inside the
+        // nomination slack; the rescoring uses the f64 envelopes.
+        const float ma = (float)pa.mean, qa = (float)pa.q, mb = (float)pb.mean, qb = (float)pb.q;
+        float ea32 = 0.0f, eb32 = 0.0f;
 #pragma unroll
-    for (int m = 0; m < 16; ++m) {
-        const int64_t i = (int64_t)row_a<G>(q, m) * kB + col;
-        const double2 v = stage[row_a<G>(q, m) * cols + c];
-        double re = 0.0, im = 0.0;
-        if (i < job.a.len) re = RAW ? v.x : env_of(v.x, pa, i);
-        if (i < job.b.len) im = RAW ? v.y : env_of(v.y, pb, i);
-        x[m] = as_point<C>(make_double2(re, im), ea, eb);
+        for (int m = 0; m < 16; ++m) {
+            const int64_t i = (int64_t)row_a<G>(q, m) * kB + col;
+            const double2 v = stage[row_a<G>(q, m) * cols + c];
+            float re = 0.0f, im = 0.0f;
+            if (i < job.a.len) re = fabsf(__fmaf_rn(2.0f, ((float)v.x - ma) - ((i & 1) ? -qa : qa), -1e-6f)) + ma;
+            if (i < job.b.len) im = fabsf(__fmaf_rn(2.0f, ((float)v.y - mb) - ((i & 1) ? -qb : qb), -1e-6f)) + mb;
+            ea32 = __fmaf_rn(re, re, ea32);
+            eb32 = __fmaf_rn(im, im, eb32);
+            x[m] = make_float2(re, im);
+        }
+        ea = ea32;
+        eb = eb32;
+    } else {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int64_t i = (int64_t)row_a<G>(q, m) * kB + col;
+            const double2 v = stage[row_a<G>(q, m) * cols + c];
+            double re = 0.0, im = 0.0;
+            if (i < job.a.len) re = RAW ? v.x : env_of(v.x, pa, i);
+            if (i < job.b.len) im = RAW ? v.y : env_of(v.y, pb, i);
+            x[m] = as_point<C>(make_double2(re, im), ea, eb);
+        }
     }
     __syncthreads();  // the stage becomes the exchange buffer
     column_group4<C, G, false>(x, 0, R / 16, q, tcol, col);
@@ -1223,20 +1244,31 @@ __global__ void __launch_bounds__(kThreads) pick_candidates(const LagJob *__rest
     for (int p = threadIdx.x; p < parts; p += blockDim.x) top = fmaxf(top, job.cands[p].top);
     top = block_max(top);
     const double floor = (double)top - slack;
-    __shared__ int count, over;
-    if (threadIdx.x == 0) count = 0, over = 0;
+    // the records at or above the floor (each holds at least one candidate,
+    // its own maximum, so more than kLagCandCap of them is an overflow)
+    __shared__ int count, over, nsel;
+    __shared__ int sel[kLagCandCap];
+    if (threadIdx.x == 0) count = 0, over = 0, nsel = 0;
     __syncthreads();
     for (int p = threadIdx.x; p < parts; p += blockDim.x) {
-        const LagCands &c = job.cands[p];
-        if ((double)c.top < floor) continue;
-        if (c.count > kLagCandCap) {
+        if ((double)job.cands[p].top < floor) continue;
+        const int k = atomicAdd(&nsel, 1);
+        if (job.cands[p].count > kLagCandCap || k >= kLagCandCap)
             over = 1;
-            continue;
-        }
-        for (int i = 0; i < c.count; ++i) {
-            if ((double)c.v[i] < floor) continue;
-            const int k = atomicAdd(&count, 1);
-            if (k < kLagCandCap) job.cand_key[k] = c.key[i];
+        else
+            sel[k] = p;
+    }
+    __syncthreads();
+    // a warp per record, its lanes over the record's candidates
+    if (!over) {
+        const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+        for (int r = threadIdx.x >> 5; r < nsel; r += warps) {
+            const LagCands &c = job.cands[sel[r]];
+            for (int i = lane; i < c.count; i += 32) {
+                if ((double)c.v[i] < floor) continue;
+                const int k = atomicAdd(&count, 1);
+                if (k < kLagCandCap) job.cand_key[k] = c.key[i];
+            }
         }
     }
     __syncthreads();
@@ -1376,24 +1408,29 @@ __device__ inline Top2 merge(Top2 a, Top2 b) {
 // The first maximum of |dot| in ascending lag (reference rescore
 // src/xcorr.zig:311-325). Where the two best are within kTieMargin (a
 // periodic signal's equal peaks), which of them the exact search picks is
-// decided by its own rounding, so the job is left to it (status 1). One
-// warp per job; parts: the job's energy records.
-__global__ void pick_rescored(const LagJob *__restrict__ jobs, int njobs, int nchunks, int parts) {
-    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (j >= njobs) return;
-    const LagJob job = jobs[j];
+// decided by its own rounding, so the job is left to it (status 1). One CTA
+// per job: a warp per candidate adds its chunk partials (lanes strided, then
+// a fixed shuffle order); parts: the job's energy records.
+__global__ void __launch_bounds__(kThreads) pick_rescored(const LagJob *__restrict__ jobs, int njobs, int nchunks,
+                                                          int parts) {
+    const LagJob job = jobs[blockIdx.x];
     if (*job.status != 0) return;
     const int count = *job.ncand;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     double e = 0.0;
-    for (int p = lane; p < parts; p += 32) e += job.energy[p].x + job.energy[p].y;
-    for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
-    e = __shfl_sync(0xffffffffu, e, 0);
-    Top2 top{Best{-INFINITY, INT64_MAX}, -INFINITY};
-    for (int c = lane; c < count; c += 32) {
+    for (int p = threadIdx.x; p < parts; p += blockDim.x) e += job.energy[p].x + job.energy[p].y;
+    e = block_sum(e);
+    __shared__ double dot[kLagCandCap];
+    for (int c = warp; c < count; c += warps) {
         double d = 0.0;
-        for (int k = 0; k < nchunks; ++k) d += job.rescore[(int64_t)c * nchunks + k];
-        top = merge(top, Top2{Best{fabs(d), (int64_t)job.cand_key[c]}, -INFINITY});
+        for (int k = lane; k < nchunks; k += 32) d += job.rescore[(int64_t)c * nchunks + k];
+        for (int off = 16; off > 0; off >>= 1) d += __shfl_down_sync(0xffffffffu, d, off);
+        if (lane == 0) dot[c] = d;
     }
+    __syncthreads();
+    if (warp != 0) return;
+    Top2 top{Best{-INFINITY, INT64_MAX}, -INFINITY};
+    for (int c = lane; c < count; c += 32) top = merge(top, Top2{Best{fabs(dot[c]), (int64_t)job.cand_key[c]}, -INFINITY});
     for (int off = 16; off > 0; off >>= 1) {
         Top2 o{Best{__shfl_down_sync(0xffffffffu, top.first.v, off), __shfl_down_sync(0xffffffffu, top.first.key, off)},
                __shfl_down_sync(0xffffffffu, top.second, off)};
@@ -1550,7 +1587,7 @@ void launch_refine_approx(const LagJob *d_job, int64_t n, int nchunks, cudaStrea
     nominate_approx<<<parts, kThreads, 0, s>>>(d_job);
     pick_candidates<<<1, kThreads, 0, s>>>(d_job, parts);
     rescore_candidates<true><<<dim3((unsigned)nchunks, 1), kThreads, 0, s>>>(d_job, nchunks);
-    pick_rescored<<<1, 32, 0, s>>>(d_job, 1, nchunks, parts);
+    pick_rescored<<<1, kThreads, 0, s>>>(d_job, 1, nchunks, parts);
     launch_counter() += 4;
 }
 
@@ -1646,7 +1683,7 @@ void launch_lag32(const LagJob *d_jobs, int njobs, int64_t n, bool raw, const fl
         rescore_candidates<true><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
     else
         rescore_candidates<false><<<dim3((unsigned)nchunks, (unsigned)njobs), kThreads, 0, s>>>(d_jobs, nchunks);
-    pick_rescored<<<(njobs + 3) / 4, 128, 0, s>>>(d_jobs, njobs, nchunks, parts);
+    pick_rescored<<<njobs, kThreads, 0, s>>>(d_jobs, njobs, nchunks, parts);
     launch_counter() += 3;
 }
 
