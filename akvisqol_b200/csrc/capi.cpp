@@ -243,13 +243,29 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
         VQB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         st.chunk_done.push_back(e);
     }
-    // chunks of about equal bytes, consecutive pairs
+    // chunks of consecutive pairs: the first L (one a lane) at front/100 of
+    // the average size, so that every lane starts scoring soon after the
+    // first uploads, and the rest of equal bytes (VISQOL_STREAMED_FRONT,
+    // default 30; 0 gives equal chunks throughout). Measured on one B200
+    // with 128 pairs of 10 s: 25-33% upload-and-score ~6% faster than equal
+    // chunks, 20% and 50% in between.
     std::vector<size_t> bounds{0};
+    size_t front = 30;
+    if (const char *env = std::getenv("VISQOL_STREAMED_FRONT")) front = (size_t)std::strtoull(env, nullptr, 10);
     {
+        std::vector<size_t> target;  // cumulative bytes at each chunk's end
+        if (front > 0 && front < 100 && K > L) {
+            const double avg = (double)total / (double)K, small = avg * (double)front / 100.0;
+            const double rest = ((double)total - small * (double)L) / (double)(K - L);
+            double at = 0.0;
+            for (size_t k = 0; k < K; ++k) target.push_back((size_t)(at += k < L ? small : rest));
+        } else {
+            for (size_t k = 0; k < K; ++k) target.push_back(total * (k + 1) / K);
+        }
         size_t acc = 0;
         for (size_t i = 0; i < n && bounds.size() < K; ++i) {
             acc += (ref_off[i] != SIZE_MAX ? up(ref_lens[i]) : 0) + (deg_off[i] != SIZE_MAX ? up(deg_lens[i]) : 0);
-            if (acc * K >= total * bounds.size() && i + 1 < n) bounds.push_back(i + 1);
+            if (acc >= target[bounds.size() - 1] && i + 1 < n) bounds.push_back(i + 1);
         }
         bounds.push_back(n);
     }
