@@ -65,11 +65,11 @@ struct LagJob {
     double *stats_a, *stats_b;
     double2 *z;          // n complex values
     int64_t *lag_out;
-    // f32 search (FP32 form): f32 transform, f64 rescoring of the near-maxima
+    // f32-nominated search: f32 transform, f64 rescoring of the near-maxima
     float2 *z32;         // n complex values
     double2 *energy;     // per forward CTA: sums of squares of a's and b's envelopes
     LagCands *cands;     // per inverse CTA
-    int32_t *status;     // 0: lag decided; 1: over kLagCandCap candidates, the f64 search decides
+    int32_t *status;     // 0: lag decided; 1: over kLagCandCap candidates or a near-tie, the f64 search decides
     int32_t *ncand;      // candidates above the job's floor
     int32_t *cand_key;   // kLagCandCap of them
     double *rescore;     // kLagCandCap x chunks partial dot products

@@ -55,7 +55,7 @@ struct PairOutcome {
     std::vector<double> grad;  // d moslqo / d degraded sample (deg_len), when requested
 };
 
-// Algorithmic DRAM bytes of one lag search (f32: the FP32 form's search).
+// Algorithmic DRAM bytes of one lag search (f32: the f32-nominated search).
 uint64_t lag_search_bytes(const LagJob &j, bool f32);
 
 struct Timing {

@@ -21,17 +21,18 @@
 //
 // The passes are written once for two complex types. double2 is the exact
 // search: every product and sum rounded separately, the CPU's results bit
-// for bit. float2 is the FP32 form's search (reference src/xcorr.zig:270-340,
-// its GPU flow src/gpu/engine.zig:445-540): the same schedule in f32 with
-// FMA, half the bytes per pass. Its correlation is within
+// for bit. float2 is the f32-nominated search every form runs (reference
+// src/xcorr.zig:270-340, its GPU flow src/gpu/engine.zig:445-540): the same
+// schedule in f32 with FMA, half the bytes per pass. Its correlation is within
 // tol(n) n (|a|^2 + |b|^2) of the exact one, tol(n) = 8 eps_f32 log2(n)
 // (src/gpu/engine.zig:820-822), so every lag whose |Re| lies within twice
 // that of the largest is nominated (each inverse CTA keeps those within the
 // slack of its own maximum, a superset), at most kLagCandCap of them per
 // search; they are rescored by f64 dot products of the envelopes and the
 // first maximum in ascending lag wins. A search with more candidates (long
-// runs of near-equal correlation: silence, periodic signals) reports it,
-// and the host reruns it with the exact search.
+// runs of near-equal correlation: silence, periodic signals), or whose two
+// best rescored lags are a near-tie, reports it, and the host reruns it with
+// the exact search, so the lag is always the exact search's.
 #include <algorithm>
 #include <cfloat>
 #include <type_traits>

@@ -129,7 +129,7 @@ void launch_fused_lag(const LagJob *d_jobs, int njobs, int64_t n, bool raw, cons
                       const double2 *tw_block, const double2 *tst, double *pv, int64_t *pk, int columns,
                       cudaStream_t s);
 
-// k_lag.cu: the FP32 form's search (fused_lag_supported(n)): the same three
+// k_lag.cu: the f32-nominated search (fused_lag_supported(n)): the same three
 // passes in f32, candidates within the f32 error bound of the maximum, f64
 // rescoring. Per job: z32 (n points), energy (lag32_parts(n)), cands
 // (lag32_parts(n)), status, ncand, cand_key (kLagCandCap), rescore

@@ -567,7 +567,8 @@ def best_lag(a, b) -> int:
 
 
 def lag_search(a, b, raw: bool = False, form: str = "exact", corr: bool = False):
-    """One pair's lag by the exact search or the FP32 form's ("fast"):
+    """One pair's lag by the f64 transform ("exact") or by the f32-nominated
+    search the batches run ("fast"):
     (lag, undecided, f32 correlation or None); see visqol_b200_lag_search."""
     a, b = mono(a, "a"), mono(b, "b")
     lag, und = c_int64(), c_int32()

@@ -241,12 +241,13 @@ int visqol_b200_best_lag(const double *a, size_t la, const double *b, size_t lb,
 
 /* The lag search of one pair in an arithmetic form: form 0 the exact f64
  * search (as visqol_b200_envelope_lag / visqol_b200_best_lag), form 1 the
- * FP32 form's: the correlation in f32, every lag within twice its error
+ * search every form's batches run: the correlation in f32, every lag within twice its error
  * bound of the maximum rescored by f64 dot products, first maximum in
  * ascending lag (reference refineLag / rescore, src/xcorr.zig:270-340, and
  * the GPU flow src/gpu/engine.zig:445-540). raw: 1 for the signals
  * themselves, 0 for their upper envelopes. *undecided (optional) is 1 when
- * the f32 pass found more than 64 candidates and the exact search decided.
+ * the f32 pass found more than 64 candidates or a near-tie and the exact
+ * search decided.
  * corr (optional, form 1): receives the f32 correlation's real part
  * (n x the circular cross-correlation, n = fftSizeFor(max(la, lb)) =
  * corr_len values). */
