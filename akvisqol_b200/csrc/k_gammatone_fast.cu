@@ -255,7 +255,7 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
     cp_async_wait_all();
     __syncthreads();
     windowed(0, 0);
-    __syncthreads();
+    if (kTileS < window) fetch(kTileS, 1);
 
     F64Pair A, B;
     F32Stage st[2];
@@ -263,13 +263,18 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
     for (int s = 0; s < 2; ++s) st[s] = F32Stage{f2(0.f), f2(0.f), f2(0.f)};
     Cascade64 CA, CB;  // kF64
     double acc_a = 0.0, acc_b = 0.0;
-    // Tile t+1's copies are in flight while tile t is filtered; its windowing
-    // waits for them (and for every thread to be done reading the buffers it
-    // overwrites, which were tile t-1's).
+    // One CTA barrier a tile. At tile t: tile t+1's copies (issued a tile
+    // earlier) are waited for; behind the barrier every thread is done
+    // filtering tile t-1 (whose windowed buffer tile t+1 takes) and done
+    // windowing tile t (whose copy buffer tile t+2 takes); then tile t+1 is
+    // windowed, tile t+2's copies are issued, and tile t is filtered.
     int buf = 0;
     for (int i0 = 0; i0 < window; i0 += kTileS) {
-        const bool more = i0 + kTileS < window;
-        if (more) fetch(i0 + kTileS, buf ^ 1);
+        const int next = i0 + kTileS;
+        if (next < window) cp_async_wait_all();
+        __syncthreads();
+        if (next < window) windowed(next, buf ^ 1);
+        if (next + kTileS < window) fetch(next + kTileS, buf);
         const int count = window - i0 < kTileS ? window - i0 : kTileS;
         if (kF64 || k.arith == kArithF64)
             filter_tile64(wx[buf], q, count, k, CA, CB);
@@ -277,12 +282,6 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
             filter_tile<true>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
         else
             filter_tile<false>(wx[buf], q, count, k, A, B, st, acc_a, acc_b);
-        if (more) {
-            cp_async_wait_all();
-            __syncthreads();
-            windowed(i0 + kTileS, buf ^ 1);
-            __syncthreads();
-        }
         buf ^= 1;
     }
     if (kF64 || k.arith == kArithF64) {
