@@ -333,10 +333,13 @@ __global__ void __launch_bounds__(W) table_staged_kernel(const TableTask *__rest
 // (reference measurePatchSimilarity, src/nsim.zig:427-510). Cell values are
 // formed from the 3x3 neighbourhood on the fly and recomputed for the
 // stddev pass (same operations, same bits).
+constexpr int kStatsCache = 64;  // a lane's cells kept between the mean and variance passes
+
 __global__ void __launch_bounds__(32) stats_kernel(const StatsJob *__restrict__ jobs, int nb) {
     const StatsJob job = jobs[blockIdx.x];
     const int r = threadIdx.x;
     __shared__ double means_sm[32];
+    __shared__ double cells_sm[kStatsCache][32];  // [column][lane]: each lane reads back its own
     int deg_col = job.deg_col;
     bool valid = true, reached = true;
     if (job.dp_offset) {
@@ -380,14 +383,21 @@ __global__ void __launch_bounds__(32) stats_kernel(const StatsJob *__restrict__ 
         double deg_sum = 0.0;
         for (int c = 0; c < nc; ++c) deg_sum += D(r, c);
         job.energy[r] = deg_sum * inv_ncols;
+        // the variance pass reuses the mean pass's cells (the same values)
+        // where they fit, instead of computing each cell twice
+        const bool cached = nc <= kStatsCache;
         double sim_sum = 0.0;
-        for (int c = 0; c < nc; ++c) sim_sum += cell(c);
+        for (int c = 0; c < nc; ++c) {
+            const double v = cell(c);
+            if (cached) cells_sm[c][r] = v;
+            sim_sum += v;
+        }
         mean = sim_sum * inv_ncols;
         double sd = 0.0;
         if (nc > 1) {
             double ss = 0.0;
             for (int c = 0; c < nc; ++c) {
-                const double diff = cell(c) - mean;
+                const double diff = (cached ? cells_sm[c][r] : cell(c)) - mean;
                 ss += diff * diff;
             }
             sd = sqrt(ss / ((double)nc - 1.0));

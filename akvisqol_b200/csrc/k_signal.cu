@@ -551,6 +551,7 @@ struct ScaleArgs {
 
 __global__ void __launch_bounds__(256) scale_kernel(const ScaleArgs *__restrict__ jobs, int njobs) {
     const ScaleArgs job = jobs[blockIdx.y];
+#pragma unroll 4
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < job.src.len;
          i += (int64_t)gridDim.x * blockDim.x)
         job.out[i] = vsig_at(job.src, i) * job.factor;
@@ -630,9 +631,11 @@ void fill_scale_args(void *dst, const VSig &src, double factor, double *out) {
 }
 void launch_scale(const void *d_args, int njobs, int64_t max_len, cudaStream_t s) {
     if (njobs <= 0) return;
+    // eight or more samples a thread: a CTA per 2048 samples, at most 256 a
+    // signal (one sample a thread made block scheduling the cost)
     const int threads = 256;
-    int64_t blocks = (max_len + threads - 1) / threads;
-    if (blocks > 2048) blocks = 2048;
+    int64_t blocks = (max_len + 8 * threads - 1) / (8 * threads);
+    if (blocks > 256) blocks = 256;
     if (blocks < 1) blocks = 1;
     scale_kernel<<<dim3((unsigned)blocks, (unsigned)njobs), threads, 0, s>>>(static_cast<const ScaleArgs *>(d_args),
                                                                             njobs);
