@@ -418,6 +418,101 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
         c->timing = c->lanes[0]->last_timing();
         return;
     }
+    // Device inputs through a chunk queue: lanes take chunks of consecutive
+    // pairs as they free up, each lane's first chunk at 30% of the average,
+    // so that the lanes fall out of step and their light phases (host
+    // planning, small kernels) overlap other lanes' heavy ones instead of
+    // coinciding. Measured on one B200 (128 pairs of 10 s): three chunks a
+    // lane score the FP32 and FP64-FMA forms ~1% faster than one share a
+    // lane; the exact form, whose lanes wait on serial sums, 6-17% slower
+    // with chunks, so it keeps one share a lane. VISQOL_DEVICE_CHUNKS
+    // overrides (chunks a lane, 0: one share a lane).
+    size_t dev_chunks = c->opt.form == vqb::kFormExact ? 0 : 3;
+    if (const char *env = std::getenv("VISQOL_DEVICE_CHUNKS")) dev_chunks = (size_t)std::strtoull(env, nullptr, 10);
+    if (device_inputs && !grads && dev_chunks > 0 && n >= dev_chunks * L) {
+        const size_t K = std::min(n, dev_chunks * L);
+        size_t total = 0;
+        for (size_t i = 0; i < n; ++i) total += ref_lens[i] + deg_lens[i];
+        std::vector<size_t> target;
+        const double avg = (double)total / (double)K, small = avg * 0.3;
+        const double rest = K > L ? ((double)total - small * (double)L) / (double)(K - L) : avg;
+        double at = 0.0;
+        for (size_t k = 0; k < K; ++k) target.push_back((size_t)(at += (K > L && k < L) ? small : rest));
+        std::vector<size_t> bounds{0};
+        size_t acc = 0;
+        for (size_t i = 0; i < n && bounds.size() < K; ++i) {
+            acc += ref_lens[i] + deg_lens[i];
+            if (acc >= target[bounds.size() - 1] && i + 1 < n) bounds.push_back(i + 1);
+        }
+        bounds.push_back(n);
+        const size_t nk = bounds.size() - 1;
+        std::atomic<size_t> next{0};
+        std::vector<std::exception_ptr> errs(L);
+        std::vector<vqb::Timing> lane_t(L);
+        auto run_chunk = [&](size_t l, size_t k) {
+            const size_t b0 = bounds[k], m = bounds[k + 1] - b0;
+            std::vector<vqb::PairOutcome> part;
+            c->lanes[l]->measure_batch(m, refs + b0, ref_lens + b0, degs + b0, deg_lens + b0, sample_rate, true, part,
+                                       prepared ? prepared + b0 : nullptr);
+            for (size_t j = 0; j < m; ++j) res[b0 + j] = std::move(part[j]);
+            const vqb::Timing &x = c->lanes[l]->last_timing();
+            vqb::Timing &a = lane_t[l];
+            a.total_ms += x.total_ms;
+            a.lag_ms += x.lag_ms;
+            a.spectrogram_ms += x.spectrogram_ms;
+            a.prep_ms += x.prep_ms;
+            a.nsim_ms += x.nsim_ms;
+            a.realign_ms += x.realign_ms;
+            a.gammatone_kernel_ms += x.gammatone_kernel_ms;
+            a.gammatone_launches += x.gammatone_launches;
+            a.gammatone_rms += x.gammatone_rms;
+            a.gammatone_window = std::max(a.gammatone_window, x.gammatone_window);
+            a.kernel_launches += x.kernel_launches;
+            a.h2d_bytes += x.h2d_bytes;
+            a.d2h_bytes += x.d2h_bytes;
+            a.host_syncs += x.host_syncs;
+        };
+        auto work = [&](size_t l) {
+            try {
+                for (size_t k = next++; k < nk; k = next++) run_chunk(l, k);
+            } catch (...) {
+                errs[l] = std::current_exception();
+            }
+        };
+        JoinAll lanes;
+        if (first_of_its_kind(c, sample_rate)) {
+            next = 1;
+            try {
+                run_chunk(0, 0);
+            } catch (...) {
+                errs[0] = std::current_exception();
+            }
+        }
+        for (size_t l = 1; l < L; ++l) lanes.threads.emplace_back(work, l);
+        work(0);
+        for (auto &th : lanes.threads) th.join();
+        for (auto &e : errs)
+            if (e) std::rethrow_exception(e);
+        vqb::Timing t{};
+        for (const vqb::Timing &x : lane_t) {
+            t.total_ms = std::max(t.total_ms, x.total_ms);
+            t.lag_ms = std::max(t.lag_ms, x.lag_ms);
+            t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
+            t.prep_ms = std::max(t.prep_ms, x.prep_ms);
+            t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
+            t.realign_ms = std::max(t.realign_ms, x.realign_ms);
+            t.gammatone_kernel_ms += x.gammatone_kernel_ms;
+            t.gammatone_launches += x.gammatone_launches;
+            t.gammatone_rms += x.gammatone_rms;
+            t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
+            t.kernel_launches += x.kernel_launches;
+            t.h2d_bytes += x.h2d_bytes;
+            t.d2h_bytes += x.d2h_bytes;
+            t.host_syncs += x.host_syncs;
+        }
+        c->timing = t;
+        return;
+    }
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {

@@ -106,3 +106,28 @@ def test_streamed_prepared(native, monkeypatch):
     for s, d in zip(streamed, direct):
         assert s["moslqo"] == d["moslqo"]
         assert np.array_equal(s["fvnsim"], d["fvnsim"])
+
+
+@pytest.mark.parametrize("precision", ["fast", "balanced"])
+def test_device_inputs_chunk_queue(native, monkeypatch, precision):
+    """Device-input batches of the FMA forms go through a queue of chunks
+    (three a lane, the first round small) that the lanes take as they free
+    up: the results are those of one share a lane and of host inputs, bit
+    for bit, in the pairs' order."""
+    from akvisqol_b200 import synth
+    pairs = synth.audio_batch(8, seed0=synth.SEED_BASE + 600, min_s=2.0, max_s=6.0)
+    refs, degs = [p[0] for p in pairs], [p[1] for p in pairs]
+    monkeypatch.setenv("VISQOL_GPU_LANES", "2")
+    ctx = native.Context(mode=native.MODE_AUDIO, precision=precision)
+    monkeypatch.setenv("VISQOL_DEVICE_CHUNKS", "3")
+    queued = _device_run(ctx, refs, degs, 48000)
+    again = _device_run(ctx, refs, degs, 48000)
+    monkeypatch.setenv("VISQOL_DEVICE_CHUNKS", "0")
+    shares = _device_run(ctx, refs, degs, 48000)
+    monkeypatch.setenv("VISQOL_STREAMED_UPLOADS", "0")
+    host = ctx.measure_batch_traced(refs, degs, 48000)
+    assert all(c == 0 for c, _, _ in queued)
+    for q, a, s, h in zip(queued, again, shares, host):
+        _same(q, s)
+        _same(a, s)
+        _same(h, s)
