@@ -179,6 +179,48 @@ bool first_of_its_kind(const visqol_ctx *c, uint32_t sample_rate) {
     return seen.insert(key).second;
 }
 
+// One lane's successive batches (chunks): spans and counts add up.
+void add_batch_timing(vqb::Timing &a, const vqb::Timing &x) {
+    a.total_ms += x.total_ms;
+    a.lag_ms += x.lag_ms;
+    a.spectrogram_ms += x.spectrogram_ms;
+    a.prep_ms += x.prep_ms;
+    a.nsim_ms += x.nsim_ms;
+    a.realign_ms += x.realign_ms;
+    a.gammatone_kernel_ms += x.gammatone_kernel_ms;
+    a.gammatone_launches += x.gammatone_launches;
+    a.gammatone_rms += x.gammatone_rms;
+    a.gammatone_window = std::max(a.gammatone_window, x.gammatone_window);
+    a.kernel_launches += x.kernel_launches;
+    a.h2d_bytes += x.h2d_bytes;
+    a.d2h_bytes += x.d2h_bytes;
+    a.host_syncs += x.host_syncs;
+    a.lag_kernel_ms += x.lag_kernel_ms;
+    a.lag_bytes += x.lag_bytes;
+    a.lag_reruns += x.lag_reruns;
+}
+
+// Lanes side by side: spans are the longest lane's, work counts add up.
+void merge_lane_timing(vqb::Timing &t, const vqb::Timing &x) {
+    t.total_ms = std::max(t.total_ms, x.total_ms);
+    t.lag_ms = std::max(t.lag_ms, x.lag_ms);
+    t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
+    t.prep_ms = std::max(t.prep_ms, x.prep_ms);
+    t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
+    t.realign_ms = std::max(t.realign_ms, x.realign_ms);
+    t.gammatone_kernel_ms += x.gammatone_kernel_ms;
+    t.gammatone_launches += x.gammatone_launches;
+    t.gammatone_rms += x.gammatone_rms;
+    t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
+    t.kernel_launches += x.kernel_launches;
+    t.h2d_bytes += x.h2d_bytes;
+    t.d2h_bytes += x.d2h_bytes;
+    t.host_syncs += x.host_syncs;
+    t.lag_kernel_ms = std::max(t.lag_kernel_ms, x.lag_kernel_ms);
+    t.lag_bytes += x.lag_bytes;
+    t.lag_reruns += x.lag_reruns;
+}
+
 // Joins the threads it holds when it goes out of scope, so that an exception
 // while starting them (a thread that cannot be created) never destroys a
 // joinable std::thread; the threads' work ends by itself.
@@ -331,22 +373,7 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
             e.measure_batch(m, d_ref.data() + b0, ref_lens + b0, d_deg.data() + b0, deg_lens + b0, sample_rate,
                             true, part, prepared ? prepared + b0 : nullptr, refs + b0);
             for (size_t j = 0; j < m; ++j) res[b0 + j] = std::move(part[j]);
-            const vqb::Timing &t = e.last_timing();
-            vqb::Timing &a = lane_t[l];
-            a.total_ms += t.total_ms;
-            a.lag_ms += t.lag_ms;
-            a.spectrogram_ms += t.spectrogram_ms;
-            a.prep_ms += t.prep_ms;
-            a.nsim_ms += t.nsim_ms;
-            a.realign_ms += t.realign_ms;
-            a.gammatone_kernel_ms += t.gammatone_kernel_ms;
-            a.gammatone_launches += t.gammatone_launches;
-            a.gammatone_rms += t.gammatone_rms;
-            a.gammatone_window = std::max(a.gammatone_window, t.gammatone_window);
-            a.kernel_launches += t.kernel_launches;
-            a.h2d_bytes += t.h2d_bytes;
-            a.d2h_bytes += t.d2h_bytes;
-            a.host_syncs += t.host_syncs;
+            add_batch_timing(lane_t[l], e.last_timing());
         } catch (...) {
             if (!errs[l]) errs[l] = std::current_exception();
             return false;
@@ -372,22 +399,7 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
     for (auto &e : errs)
         if (e) std::rethrow_exception(e);
     vqb::Timing t{};
-    for (const vqb::Timing &x : lane_t) {
-        t.total_ms = std::max(t.total_ms, x.total_ms);
-        t.lag_ms = std::max(t.lag_ms, x.lag_ms);
-        t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
-        t.prep_ms = std::max(t.prep_ms, x.prep_ms);
-        t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
-        t.realign_ms = std::max(t.realign_ms, x.realign_ms);
-        t.gammatone_kernel_ms += x.gammatone_kernel_ms;
-        t.gammatone_launches += x.gammatone_launches;
-        t.gammatone_rms += x.gammatone_rms;
-        t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
-        t.kernel_launches += x.kernel_launches;
-        t.h2d_bytes += x.h2d_bytes;
-        t.d2h_bytes += x.d2h_bytes;
-        t.host_syncs += x.host_syncs;
-    }
+    for (const vqb::Timing &x : lane_t) merge_lane_timing(t, x);
     for (size_t i = 0; i < n; ++i)
         t.h2d_bytes += (d_ref[i] ? ref_lens[i] : 0) * sizeof(double) + (d_deg[i] ? deg_lens[i] : 0) * sizeof(double);
     c->timing = t;
@@ -455,22 +467,7 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
             c->lanes[l]->measure_batch(m, refs + b0, ref_lens + b0, degs + b0, deg_lens + b0, sample_rate, true, part,
                                        prepared ? prepared + b0 : nullptr);
             for (size_t j = 0; j < m; ++j) res[b0 + j] = std::move(part[j]);
-            const vqb::Timing &x = c->lanes[l]->last_timing();
-            vqb::Timing &a = lane_t[l];
-            a.total_ms += x.total_ms;
-            a.lag_ms += x.lag_ms;
-            a.spectrogram_ms += x.spectrogram_ms;
-            a.prep_ms += x.prep_ms;
-            a.nsim_ms += x.nsim_ms;
-            a.realign_ms += x.realign_ms;
-            a.gammatone_kernel_ms += x.gammatone_kernel_ms;
-            a.gammatone_launches += x.gammatone_launches;
-            a.gammatone_rms += x.gammatone_rms;
-            a.gammatone_window = std::max(a.gammatone_window, x.gammatone_window);
-            a.kernel_launches += x.kernel_launches;
-            a.h2d_bytes += x.h2d_bytes;
-            a.d2h_bytes += x.d2h_bytes;
-            a.host_syncs += x.host_syncs;
+            add_batch_timing(lane_t[l], c->lanes[l]->last_timing());
         };
         auto work = [&](size_t l) {
             try {
@@ -494,22 +491,7 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
         for (auto &e : errs)
             if (e) std::rethrow_exception(e);
         vqb::Timing t{};
-        for (const vqb::Timing &x : lane_t) {
-            t.total_ms = std::max(t.total_ms, x.total_ms);
-            t.lag_ms = std::max(t.lag_ms, x.lag_ms);
-            t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
-            t.prep_ms = std::max(t.prep_ms, x.prep_ms);
-            t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
-            t.realign_ms = std::max(t.realign_ms, x.realign_ms);
-            t.gammatone_kernel_ms += x.gammatone_kernel_ms;
-            t.gammatone_launches += x.gammatone_launches;
-            t.gammatone_rms += x.gammatone_rms;
-            t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
-            t.kernel_launches += x.kernel_launches;
-            t.h2d_bytes += x.h2d_bytes;
-            t.d2h_bytes += x.d2h_bytes;
-            t.host_syncs += x.host_syncs;
-        }
+        for (const vqb::Timing &x : lane_t) merge_lane_timing(t, x);
         c->timing = t;
         return;
     }
@@ -556,25 +538,7 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
     vqb::Timing t{};
     for (size_t l = 0; l < L; ++l) {
         for (size_t k = 0; k < part[l].size(); ++k) res[part[l][k]] = std::move(lane_out[l][k]);
-        const vqb::Timing &x = c->lanes[l]->last_timing();
-        // lanes overlap: spans are the longest lane's, work counts add up
-        t.total_ms = std::max(t.total_ms, x.total_ms);
-        t.lag_ms = std::max(t.lag_ms, x.lag_ms);
-        t.spectrogram_ms = std::max(t.spectrogram_ms, x.spectrogram_ms);
-        t.prep_ms = std::max(t.prep_ms, x.prep_ms);
-        t.nsim_ms = std::max(t.nsim_ms, x.nsim_ms);
-        t.realign_ms = std::max(t.realign_ms, x.realign_ms);
-        t.gammatone_kernel_ms += x.gammatone_kernel_ms;
-        t.gammatone_launches += x.gammatone_launches;
-        t.gammatone_rms += x.gammatone_rms;
-        t.gammatone_window = std::max(t.gammatone_window, x.gammatone_window);
-        t.kernel_launches += x.kernel_launches;
-        t.h2d_bytes += x.h2d_bytes;
-        t.d2h_bytes += x.d2h_bytes;
-        t.host_syncs += x.host_syncs;
-        t.lag_kernel_ms = std::max(t.lag_kernel_ms, x.lag_kernel_ms);
-        t.lag_bytes += x.lag_bytes;
-        t.lag_reruns += x.lag_reruns;
+        merge_lane_timing(t, c->lanes[l]->last_timing());
     }
     c->timing = t;
 }

@@ -214,11 +214,7 @@ __device__ __forceinline__ void fast_tile(const Tile tile, const SpecJob *__rest
                                           double (*raw)[kCtaFrames][kTileS], double (*wx)[kTileS][kRowPad]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int groups = (nb + 7) >> 3;
-    // Warp w issues on SM sub-partition w % 4. The band group rotates with
-    // the frame block so that the lowest group's warps (all-f64 cascades, the
-    // heaviest) sit on different sub-partitions instead of sharing one
-    // (measured 0.433 against 0.424 of the FP32 peak).
-    const int fblock = warp / groups, g = (warp + fblock) % groups;
+    const int g = warp % groups, fblock = warp / groups;
     const int band_raw = g * 8 + (lane & 7);
     const int band = band_raw < nb ? band_raw : nb - 1;  // idle lanes filter a real band, never write
     const int q = fblock * kFramesPerBlock + 2 * (lane >> 3);
