@@ -1113,9 +1113,12 @@ __global__ void __launch_bounds__(kThreads) inv_columns_nominate(const LagJob *_
     block_nominate(v, key, slack, job.cands + blockIdx.x);
 }
 
-// Pass 3 of the f32 search, register form (4 <= G <= 11).
+// Pass 3 of the f32 search, register form (4 <= G <= 11). Four CTAs an SM
+// (64 registers, no spills; 32 KB of exchange buffer each): the pass reads
+// its 4096 points at once and then only computes, so more resident CTAs keep
+// more loads in flight.
 template <int G>
-__global__ void __launch_bounds__(kThreads, 3) inv_columns_reg_nominate(const LagJob *__restrict__ jobs,
+__global__ void __launch_bounds__(kThreads, 4) inv_columns_reg_nominate(const LagJob *__restrict__ jobs,
                                                                      const float2 *__restrict__ tcol, int parts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2 *sm = reinterpret_cast<float2 *>(smem_raw);
