@@ -291,26 +291,12 @@ bool run_lanes_queued(visqol_ctx *c, size_t n, const double *const *refs, const 
     // default 30; 0 gives equal chunks throughout). Measured on one B200
     // with 128 pairs of 10 s: 25-33% upload-and-score ~6% faster than equal
     // chunks, 20% and 50% in between.
-    std::vector<size_t> bounds{0};
     size_t front = 30;
     if (const char *env = std::getenv("VISQOL_STREAMED_FRONT")) front = (size_t)std::strtoull(env, nullptr, 10);
-    {
-        std::vector<size_t> target;  // cumulative bytes at each chunk's end
-        if (front > 0 && front < 100 && K > L) {
-            const double avg = (double)total / (double)K, small = avg * (double)front / 100.0;
-            const double rest = ((double)total - small * (double)L) / (double)(K - L);
-            double at = 0.0;
-            for (size_t k = 0; k < K; ++k) target.push_back((size_t)(at += k < L ? small : rest));
-        } else {
-            for (size_t k = 0; k < K; ++k) target.push_back(total * (k + 1) / K);
-        }
-        size_t acc = 0;
-        for (size_t i = 0; i < n && bounds.size() < K; ++i) {
-            acc += (ref_off[i] != SIZE_MAX ? up(ref_lens[i]) : 0) + (deg_off[i] != SIZE_MAX ? up(deg_lens[i]) : 0);
-            if (acc >= target[bounds.size() - 1] && i + 1 < n) bounds.push_back(i + 1);
-        }
-        bounds.push_back(n);
-    }
+    std::vector<size_t> sizes(n);
+    for (size_t i = 0; i < n; ++i)
+        sizes[i] = (ref_off[i] != SIZE_MAX ? up(ref_lens[i]) : 0) + (deg_off[i] != SIZE_MAX ? up(deg_lens[i]) : 0);
+    const std::vector<size_t> bounds = vqb::host::chunk_bounds(sizes, K, L, front);
     const size_t nk = bounds.size() - 1;
     char *base = reinterpret_cast<char *>(st.buf);
     std::vector<const double *> d_ref(n, nullptr), d_deg(n, nullptr);
@@ -440,23 +426,12 @@ void run_lanes(visqol_ctx *c, size_t n, const double *const *refs, const size_t 
     // with chunks, so it keeps one share a lane. VISQOL_DEVICE_CHUNKS
     // overrides (chunks a lane, 0: one share a lane).
     size_t dev_chunks = c->opt.form == vqb::kFormExact ? 0 : 3;
-    if (const char *env = std::getenv("VISQOL_DEVICE_CHUNKS")) dev_chunks = (size_t)std::strtoull(env, nullptr, 10);
+    if (const char *env = std::getenv("VISQOL_DEVICE_CHUNKS"))
+        dev_chunks = std::min<size_t>(16, (size_t)std::strtoull(env, nullptr, 10));
     if (device_inputs && !grads && dev_chunks > 0 && n >= dev_chunks * L) {
-        const size_t K = std::min(n, dev_chunks * L);
-        size_t total = 0;
-        for (size_t i = 0; i < n; ++i) total += ref_lens[i] + deg_lens[i];
-        std::vector<size_t> target;
-        const double avg = (double)total / (double)K, small = avg * 0.3;
-        const double rest = K > L ? ((double)total - small * (double)L) / (double)(K - L) : avg;
-        double at = 0.0;
-        for (size_t k = 0; k < K; ++k) target.push_back((size_t)(at += (K > L && k < L) ? small : rest));
-        std::vector<size_t> bounds{0};
-        size_t acc = 0;
-        for (size_t i = 0; i < n && bounds.size() < K; ++i) {
-            acc += ref_lens[i] + deg_lens[i];
-            if (acc >= target[bounds.size() - 1] && i + 1 < n) bounds.push_back(i + 1);
-        }
-        bounds.push_back(n);
+        std::vector<size_t> sizes(n);
+        for (size_t i = 0; i < n; ++i) sizes[i] = ref_lens[i] + deg_lens[i];
+        const std::vector<size_t> bounds = vqb::host::chunk_bounds(sizes, dev_chunks * L, L, 30);
         const size_t nk = bounds.size() - 1;
         std::atomic<size_t> next{0};
         std::vector<std::exception_ptr> errs(L);

@@ -625,5 +625,30 @@ std::vector<double> decode_wav(const std::string &bytes, uint32_t *sample_rate) 
     return out;
 }
 
+std::vector<size_t> chunk_bounds(const std::vector<size_t> &sizes, size_t chunks, size_t lanes, size_t front) {
+    const size_t n = sizes.size();
+    std::vector<size_t> bounds{0};
+    if (n == 0) return bounds;
+    const size_t K = std::max<size_t>(1, std::min(n, chunks));
+    size_t total = 0;
+    for (size_t s : sizes) total += s;
+    std::vector<size_t> target;  // cumulative size at each chunk's end
+    if (front > 0 && front < 100 && K > lanes) {
+        const double avg = (double)total / (double)K, small = avg * (double)front / 100.0;
+        const double rest = ((double)total - small * (double)lanes) / (double)(K - lanes);
+        double at = 0.0;
+        for (size_t k = 0; k < K; ++k) target.push_back((size_t)(at += k < lanes ? small : rest));
+    } else {
+        for (size_t k = 0; k < K; ++k) target.push_back((size_t)((double)total * (double)(k + 1) / (double)K));
+    }
+    size_t acc = 0;
+    for (size_t i = 0; i + 1 < n && bounds.size() < K; ++i) {
+        acc += sizes[i];
+        if (acc >= target[bounds.size() - 1]) bounds.push_back(i + 1);
+    }
+    bounds.push_back(n);
+    return bounds;
+}
+
 }  // namespace host
 }  // namespace vqb

@@ -156,5 +156,14 @@ Scores build_scores(std::vector<Match> matches, size_t nb, double frame_duration
 std::vector<double> decode_wav(const std::string &bytes, uint32_t *sample_rate);
 std::string read_file(const std::string &path);
 
+// A batch cut into at most `chunks` runs of consecutive pairs by size (a
+// pair's samples or bytes, `sizes`), for the lanes' chunk queues: the first
+// `lanes` chunks at front/100 of the average size, so that every lane starts
+// soon, the rest of equal size (front 0 or >= 100, or no more chunks than
+// lanes: equal sizes throughout). Returns the bounds 0 = b0 < b1 < ... = n,
+// every chunk holding at least one pair (fewer chunks where single pairs
+// span several targets); {0} for an empty batch.
+std::vector<size_t> chunk_bounds(const std::vector<size_t> &sizes, size_t chunks, size_t lanes, size_t front);
+
 }  // namespace host
 }  // namespace vqb

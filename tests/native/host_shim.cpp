@@ -105,4 +105,11 @@ int64_t hs_decode_wav(const char *bytes, size_t n, double *out, size_t cap, uint
     }
 }
 
+// out holds n + 1 entries; returns the number of bounds written.
+size_t hs_chunk_bounds(const size_t *sizes, size_t n, size_t chunks, size_t lanes, size_t front, size_t *out) {
+    const auto b = host::chunk_bounds(std::vector<size_t>(sizes, sizes + n), chunks, lanes, front);
+    std::memcpy(out, b.data(), b.size() * sizeof(size_t));
+    return b.size();
+}
+
 }  // extern "C"

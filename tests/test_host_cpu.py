@@ -1,5 +1,5 @@
 """The product's host-side model (filter design, planning, SPL, SVR, WAV)
-against the oracle, on the CPU: compiled from akvisqol_b200/csrc/host_model.cpp
+against the oracle, and the lanes' chunk planning against its rule, on the CPU: compiled from akvisqol_b200/csrc/host_model.cpp
 into a test library with a thin C shim (tests/native/host_shim.cpp)."""
 
 import ctypes
@@ -46,6 +46,7 @@ def hs():
         ("hs_spl_factor", c_double, [c_double, c_size_t, c_double, c_size_t]),
         ("hs_svr_predict", c_int, [c_char_p, c_size_t, D, D]),
         ("hs_decode_wav", c_int64, [c_char_p, c_size_t, D, c_size_t, POINTER(c_uint32)]),
+        ("hs_chunk_bounds", c_size_t, [SZ, c_size_t, c_size_t, c_size_t, c_size_t, SZ]),
     ]:
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
@@ -209,3 +210,65 @@ def test_decode_wav(hs):
     assert hs.hs_decode_wav(w, len(w), d(out), 16, ctypes.byref(rate)) == 2
     assert out[0] == 0.5 and out[1] == -0.25
     assert hs.hs_decode_wav(b"RIFX0000WAVE", 12, d(out), 16, ctypes.byref(rate)) == -3
+
+
+def _bounds(hs, sizes, chunks, lanes, front):
+    s = np.ascontiguousarray(sizes, dtype=np.uintp)
+    out = np.zeros(len(s) + 1, dtype=np.uintp)
+    k = hs.hs_chunk_bounds(s.ctypes.data_as(POINTER(c_size_t)), len(s), chunks, lanes, front,
+                           out.ctypes.data_as(POINTER(c_size_t)))
+    return out[:k].tolist()
+
+
+def test_chunk_bounds_cases(hs):
+    """The lanes' chunk queues (host and device inputs): consecutive pairs cut
+    at cumulative size targets, the first `lanes` chunks at front% of the
+    average."""
+    assert _bounds(hs, [], 6, 2, 30) == [0]
+    assert _bounds(hs, [7], 6, 2, 30) == [0, 1]
+    assert _bounds(hs, [1] * 10, 5, 1, 0) == [0, 2, 4, 6, 8, 10]
+    assert _bounds(hs, [1] * 10, 5, 1, 100) == [0, 2, 4, 6, 8, 10]
+    # 100 equal pairs, 10 chunks over 5 lanes: average 10, the first five at 3,
+    # the other five at (100 - 15) / 5 = 17
+    assert _bounds(hs, [1] * 100, 10, 5, 30) == [0, 3, 6, 9, 12, 15, 32, 49, 66, 83, 100]
+    # no more chunks than lanes: equal chunks whatever the front
+    assert _bounds(hs, [1] * 12, 4, 4, 30) == [0, 3, 6, 9, 12]
+    # a large pair first passes several targets but makes one chunk
+    assert _bounds(hs, [100, 1, 1, 1], 4, 2, 0) == [0, 1, 2, 3, 4]
+    # a large pair last: the small ones reach no target, one chunk
+    assert _bounds(hs, [1, 1, 1, 100], 4, 1, 0) == [0, 4]
+    assert _bounds(hs, [0, 0, 0], 3, 1, 30) == [0, 1, 2, 3]
+    assert _bounds(hs, [5, 5], 8, 2, 30) == [0, 1, 2]
+
+
+def test_chunk_bounds_properties(hs):
+    rng = np.random.default_rng(5)
+    for _ in range(300):
+        n = int(rng.integers(1, 200))
+        sizes = rng.integers(0, 1 << 24, n)
+        if rng.random() < 0.2:
+            sizes[rng.integers(n)] = 1 << 30
+        lanes = int(rng.integers(1, 9))
+        chunks = int(rng.integers(1, 4 * lanes + 1))
+        front = int(rng.choice([0, 10, 30, 50, 99, 100, 150]))
+        b = _bounds(hs, sizes, chunks, lanes, front)
+        assert b[0] == 0 and b[-1] == n
+        assert all(x < y for x, y in zip(b, b[1:])), b
+        assert len(b) - 1 <= min(n, chunks)
+        # the greedy rule: a chunk ends at the first pair whose running total
+        # reaches that chunk's target, so no chunk ends early
+        K = min(n, chunks)
+        total = float(sizes.sum())
+        if 0 < front < 100 and K > lanes:
+            small = total / K * front / 100
+            rest = (total - small * lanes) / (K - lanes)
+            steps = [small if k < lanes else rest for k in range(K)]
+        else:
+            steps = [total / K] * K
+        acc = np.cumsum(sizes)
+        at = 0.0
+        for k, e in enumerate(b[1:-1]):
+            at += steps[k]
+            assert acc[e - 1] >= int(at) - 1, (k, e)
+            if e - 1 > b[k]:
+                assert acc[e - 2] < int(at) + 1, (k, e)
